@@ -1,0 +1,343 @@
+"""Benchmark of the DEM step: particle-steps/s at 1M spheres.
+
+Workload: the 1,048,576-sphere box scene (log-normal radii, median 0.002,
+sigma 0.25, clipped to [0.001, 0.004]; box 1 x 1 x 4; spring 5e4, sphere
+restitution 0.4, walls 0.7, dt 5e-6; grid cell 2 r_max -> 126 x 126 x 501
+cells), FP32, one simulation per GPU.  A bench "step" is one simulation step
+of all particles: integrate, walls, grid rebuild, contacts.
+
+Under the reference's scheme the contact kick is not scaled by dt, and with
+this scene's spring and its smallest spheres the explicit update is unstable:
+velocities diverge within a few steps and NaN appears after about a hundred.
+Every timed block of --block steps therefore starts from the scene's
+initial state, restored from an on-device checkpoint outside the timed
+region, so all timed steps are steps 1..block of the scene.
+
+Reports one JSON line (rank 0): value = device time (CUDA events on the
+library's stream) of exactly --steps steps, max over ranks; e2e = the same
+steps through host buffers (upload, steps, download per block); roofline of
+the dominant kernel from a per-kernel event pass; cpu_baseline = the
+reference's own CPU simulator on a bounded sample.
+
+--impl reference times the reference's CPU simulator (oracle/_ref, built
+from the reference sources) on the same scene and prints its line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "particle-stabilizer_b200", "python"))
+
+METRIC = "particle-steps/s at 1M spheres (forward)"
+UNIT = "particle-steps/s"
+WORKLOAD = ("1,048,576 spheres, log-normal r (median 0.002, sigma 0.25, clip [0.001,0.004]), box 1x1x4, "
+            "k 5e4, e 0.4, walls 0.7, dt 5e-6, cell 2 r_max")
+L2_BYTES = 126 * 2 ** 20
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        time.sleep(0.25)
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+            os.unlink(self.path)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# algorithmic bytes per particle of each kernel (FP32 state = 2 x 16 B)
+def alg_bytes(kind: str, n: int, cells: int, vb: int = 16) -> float:
+    st = 2 * vb
+    return {
+        "contacts": n * (st + st + 8),          # own state in, next state out, cell+slot out
+        "rank_move": n * (st + 8 + 4 + st + 4),  # state, cell+slot, own tmp in; state, orig out
+        "scatter": n * (12 + 4),                # cell, slot, orig in; tmp out
+        "scan": cells * 8,                      # counts in, offsets out
+        "begin": n * (st + st + 8),
+    }[kind]
+
+
+def step_alg_bytes(n: int, cells: int) -> float:
+    """Whole-step algorithmic bytes: 128 B per particle (two passes over the
+    32-B state, in and out) + 4 B per cell."""
+    return 128.0 * n + 4.0 * cells
+
+
+def reference_cpu_sample(scene, budget_s: float, max_steps: int, warmup: int = 0) -> dict:
+    """The reference's own CPU simulator (oracle/_ref/libref_cpu.so) on the
+    same scene: construction and `warmup` steps untimed, then whole steps
+    until the budget or max_steps."""
+    from oracle import ps_oracle as O
+
+    if os.path.exists(O.REF_CPU_SO):
+        r = O.ref_cpu()
+        kind = "reference"
+    else:
+        r = None
+        kind = "port"
+    if r is not None:
+        h = r.create(scene)
+        if warmup > 0:
+            r.step(h, warmup)
+        steps, t = 0, 0.0
+        while steps < max_steps and t < budget_s:
+            t += r.time_steps(h, 1)
+            steps += 1
+        r.destroy(h)
+    else:
+        # the oracle (C restatement of the same scheme), one thread
+        t0 = time.perf_counter()
+        steps = 0
+        st = scene
+        while steps < max_steps and time.perf_counter() - t0 < budget_s:
+            O.run(st, 1, "f64")
+            steps += 1
+        t = time.perf_counter() - t0
+    return {"value": scene.n * steps / t, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{steps} full steps of the 1M-sphere scene from its initial state "
+                      f"({t:.1f} s, one thread: the reference's box path is serial)",
+            "seconds": t, "steps": steps}
+
+
+def run_ours(args, world, rank, local, dist):
+    import psb200
+    from psb200 import scenes
+
+    sc = scenes.c2_scene()
+    n = sc.n
+    sim = psb200.Simulation(sc, args.precision, device=local)
+    sim.set_state()
+    sim.checkpoint_save(0)
+    g = sim.grid(0)
+    cells = int(g.n_cells)
+    block = max(1, args.block)
+
+    def timed_steps(total: int) -> tuple[float, int]:
+        ms, launches, left = 0.0, 0, total
+        while left > 0:
+            b = min(block, left)
+            sim.checkpoint_load(0)
+            ms += sim.time_steps(b)
+            launches += sim.launches()
+            left -= b
+        return ms, launches
+
+    timed_steps(max(args.warmup, 3))
+    barrier(dist)
+    sim.sync()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        dev_ms, launches = timed_steps(args.steps)
+        sim.sync()
+        wall = time.perf_counter() - t0
+    barrier(dist)
+    dev_ms_max = max_over_ranks(dist, dev_ms)
+    total_particle_steps = sum_over_ranks(dist, float(n * args.steps))
+    value = total_particle_steps / (dev_ms_max * 1e-3)
+
+    # per-kernel device times (eager launches, events around each) over one block
+    sim.checkpoint_load(0)
+    prof = sim.profile_steps(min(block, args.steps))
+    per_step = {k: (ms / max(1, min(block, args.steps)), cnt) for k, (ms, cnt) in prof.items()}
+    dom = max(("contacts", "rank_move", "scatter", "scan"), key=lambda k: prof[k][0])
+    dom_ms_avg = prof[dom][0] / max(1, prof[dom][1])
+    peak, peak_kind = peaks()
+    achieved = alg_bytes(dom, n, cells) / (dom_ms_avg * 1e-3) / 1e9
+    step_ms = dev_ms / args.steps
+    step_gbs = step_alg_bytes(n, cells) / (step_ms * 1e-3) / 1e9
+
+    # end to end through host buffers: upload, block steps, download
+    e2e_iters = max(1, min(args.steps // block, 5))
+    host = np.ascontiguousarray(sc.state)
+    t_e2e = 0.0
+    for _ in range(e2e_iters + 1):
+        t0 = time.perf_counter()
+        sim.set_state(host)
+        sim.step(block)
+        out = sim.get_state()
+        dt = time.perf_counter() - t0
+        if _ > 0:  # first iteration warms the upload path
+            t_e2e += dt
+    e2e_value = sum_over_ranks(dist, float(n * block * e2e_iters)) / max_over_ranks(dist, t_e2e)
+    del out
+
+    state_bytes = n * (4 * 2 * 16 + 4 * 4) + 2 * 4 * (cells + 1)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "f32" else "f64",
+        "data": "synthetic: seeded generator of the 1M-sphere scene (numpy default_rng(2))",
+        "config": {"workload": WORKLOAD, "n_particles": n, "grid": [g.nb[0], g.nb[1], g.nb[2]], "cells": cells,
+                   "block": block, "state_restored_every": block,
+                   "l2": f"working set {state_bytes / 2**20:.0f} MiB > 126 MiB L2; no flush",
+                   "parallelism": f"{world} independent replicas (one per GPU, no collective)"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "alg_bytes_per_launch": alg_bytes(dom, n, cells)},
+        "step_roofline": {"alg_bytes_per_step": step_alg_bytes(n, cells), "achieved_gbs": step_gbs,
+                          "frac": step_gbs / peak},
+        "kernels_ms_per_step": {k: v[0] for k, v in per_step.items()},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 64.0 * n / block,
+                "d2h_bytes_per_step": 64.0 * n / block,
+                "how": f"ps_set_state(host) + ps_step({block}) + ps_get_state(host), wall clock, {e2e_iters} blocks"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "wall_s": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = reference_cpu_sample(sc, args.cpu_budget, 20)
+    sim.close()
+    return line
+
+
+def run_reference(args, world, rank):
+    """Reference arm: the reference's own CPU simulator on the same scene."""
+    from psb200 import scenes
+
+    if rank != 0:
+        return None
+    sc = scenes.c2_scene()
+    s = reference_cpu_sample(sc, args.cpu_budget, max(1, args.steps), warmup=min(args.warmup, 1))
+    return {"impl": "reference", "metric": METRIC, "value": s["value"], "unit": UNIT, "n_gpus": world,
+            "steps": s["steps"], "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * s["seconds"] / s["steps"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded generator of the 1M-sphere scene (numpy default_rng(2))",
+            "config": {"workload": WORKLOAD, "n_particles": sc.n,
+                       "note": f"{s['steps']} of the requested {args.steps} steps fit the time budget"},
+            "cpu_baseline": {k: s[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": s["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--block", type=int, default=100, help="steps per block; the state is restored between blocks")
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference CPU stepping")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # rank 0 alone times the reference's CPU simulator; other ranks exit
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        line = run_reference(args, world, rank)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    world, rank, local, dist = dist_setup()
+    if True:
+        line = run_ours(args, world, rank, local, dist)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,193 @@
+/*
+ * particle_stabilizer_b200.h — C ABI of libparticle_stabilizer_cuda.so, the
+ * B200 (sm_100a) implementation of particle-stabilizer's per-step DEM path.
+ *
+ * Plain C types only: pointers, sizes, int status codes.  Every function
+ * returns PS_OK (0) or a negative PS_ERR_* code; ps_last_error() gives the
+ * message of the calling thread's last failure.  Nothing here exits the
+ * process (the reference's CUDA_CHECK_ERROR logs and calls exit(),
+ * include/ParticleStabilizerCUDA/CudaCommon.cuh:18-28).
+ *
+ * Host state layout (AoS, 8 doubles per particle, the reference's
+ * ParticlePrimitive<glm::dvec3>, include/ParticleStabilizer/ParticleModel.hpp:7-25):
+ *   x, y, z, vx, vy, vz, radius, mass
+ *
+ * The library also exports the reference's own entry point
+ *   extern "C" void runSimulateCUDA(...)
+ * with the exact C++ signature of
+ * include/ParticleStabilizerCUDA/PhysicsEngineCUDA.hpp:43-54; it is declared
+ * in include/ps_runsimulate.hpp because its arguments are C++ types.
+ */
+#ifndef PARTICLE_STABILIZER_B200_H
+#define PARTICLE_STABILIZER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PS_OK 0
+#define PS_ERR_INVALID (-1)      /* bad argument                                */
+#define PS_ERR_CUDA (-2)         /* CUDA runtime error                          */
+#define PS_ERR_NOMEM (-3)        /* device or host allocation failed            */
+#define PS_ERR_DEVICE (-4)       /* a kernel raised its device error word       */
+#define PS_ERR_IO (-5)           /* file could not be read or written           */
+
+#define PS_FP32 0
+#define PS_FP64 1
+
+/* Wall restitution indices, in the reference's order
+ * (include/ParticleStabilizer/ContainerBase.hpp:10-34). */
+#define PS_ZMIN 0
+#define PS_ZMAX 1
+#define PS_XMIN 2
+#define PS_XMAX 3
+#define PS_YMIN 4
+#define PS_YMAX 5
+
+/* One scene: the arguments of runSimulateCUDA
+ * (src/ParticleStabilizerCUDA/PhysicsEngineCUDA.cpp:86-97) minus the state. */
+typedef struct ps_scene_desc {
+  int64_t n_particles;
+  double box_min[3];        /* box container (ignored when tri != NULL)        */
+  double box_max[3];
+  double gravity[3];
+  double e_wall[6];         /* PS_ZMIN..PS_YMAX                                 */
+  double k_spring;          /* coefficientOfSpring                              */
+  double e_sphere;          /* coefficientOfRestitutionSphere                   */
+  double dt;
+  double cell_size;         /* grid cell edge; 0 = reference rule 2.0*1.05*r_max
+                               (ParticleModelCUDA.cpp:84); must be >= 2*r_max   */
+  const double* tri;        /* triangle container: 9 doubles per triangle
+                               (de-indexed soup, PolygonContainerCUDA.cpp:35-53);
+                               NULL = box                                        */
+  int64_t n_tri;
+  int32_t edge_quirk;       /* 1 = the reference's edge pick by dot(center, point)
+                               (PolygonContainerCUDA_kernels.cu:130-150); 0 = true
+                               nearest edge point                                */
+  int32_t widen_domain;     /* triangle container: grid domain = mesh AABB union
+                               initial particle AABB (the reference uses the mesh
+                               AABB only, PhysicsEngineCUDA.cpp:117)             */
+} ps_scene_desc;
+
+typedef struct ps_stats {    /* ParticleStatisticsCUDA (ParticleStatisticsCUDA.hpp:9-24) */
+  double kinetic_energy;     /* sum 0.5 m |v|^2, FP64 reduction                   */
+  double min_pos[3];         /* min of centre - radius                            */
+  double max_pos[3];         /* max of centre + radius                            */
+  int64_t n_collided;        /* particles overlapping a higher-indexed particle   */
+  double max_overlap;        /* max over pairs of r_i + r_j - |x_i - x_j|         */
+} ps_stats;
+
+typedef struct ps_grid_info {
+  double min[3];             /* grid domain minimum                              */
+  double interval;           /* cell edge                                        */
+  int32_t nb[3];             /* cells per axis                                    */
+  int64_t n_cells;
+  int64_t cell_base;         /* first global cell id of this scene               */
+  int64_t particle_base;     /* first particle slot of this scene                */
+} ps_grid_info;
+
+typedef struct ps_sim ps_sim;
+
+/* Message of this thread's last failure ("" if none). */
+const char* ps_last_error(void);
+
+/* Create a simulation of n_scenes independent scenes on CUDA device
+ * `device`, in PS_FP32 or PS_FP64.  One scene replaces the set-up half of
+ * runSimulateCUDA: ParticleModelCUDA ctor + container ctor + initBuckets
+ * (PhysicsEngineCUDA.cpp:98-117, ParticleModelCUDA.cpp:4-52,62-113).
+ * Several scenes advance together in every launch (batched execution).
+ * The grid's r_max is taken from the first ps_set_state. */
+int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t precision, int32_t device, ps_sim** out);
+
+/* Upload host state, scenes concatenated in order (replaces the H2D copy
+ * of ParticleModelCUDA.cpp:36-43).  Also sizes the grids on first call. */
+int ps_set_state(ps_sim* sim, const double* aos, int64_t n_total);
+
+/* Download state in original particle order (ParticleModelCUDA::getParticles,
+ * ParticleModelCUDA.cpp:183-189, and the copy-back of PhysicsEngineCUDA.cpp:154-174). */
+int ps_get_state(ps_sim* sim, double* aos_out, int64_t n_total);
+
+/* Advance every scene by n_steps steps (the loop body of
+ * PhysicsEngineCUDA::startSimulationLoop, PhysicsEngineCUDA.cpp:38-42).
+ * Asynchronous on the simulation's stream; blocks of steps run as CUDA graphs. */
+int ps_step(ps_sim* sim, int64_t n_steps);
+
+/* Wait for the stream and check the device error word. */
+int ps_sync(ps_sim* sim);
+
+/* Statistics of one scene (ParticleStatisticsCUDA::calculateStatistics,
+ * ParticleStatisticsCUDA.cpp:11-62), using the grid instead of O(N^2). */
+int ps_stats_get(ps_sim* sim, int32_t scene, ps_stats* out);
+
+/* Grid of one scene (BucketContext, ParticleModelCUDA.hpp:17-32). */
+int ps_grid_get(ps_sim* sim, int32_t scene, ps_grid_info* out);
+
+/* Bucket arrays of the last grid rebuild over all scenes: per-cell counts
+ * and exclusive offsets (n_cells_total entries each; the reference's
+ * _deviceBucketCounter and _deviceBucketCumsumCounter), and the particle
+ * index list in canonical order (cells ascending, original index ascending
+ * inside a cell; the reference's _deviceBucket, ParticleModelCUDA.cpp:115-155).
+ * Any pointer may be NULL. */
+int ps_buckets_get(ps_sim* sim, uint32_t* counts, uint32_t* offsets, uint32_t* order);
+
+/* Number of kernel launches issued by the last ps_step. */
+int64_t ps_last_launch_count(ps_sim* sim);
+
+/* Device-side checkpoints of the at-rest state (positions, velocities,
+ * particle order) in numbered slots, kept in device memory.  No counterpart
+ * in the reference (it has no checkpointing); used for restarts, the
+ * checkpointed backward pass and benchmarking from a fixed state.
+ * Ordered on the simulation's stream. */
+int ps_checkpoint_save(ps_sim* sim, int32_t slot);
+int ps_checkpoint_load(ps_sim* sim, int32_t slot);
+
+/* Measurement (no counterpart in the reference, whose host loop syncs after
+ * every launch): ps_time_steps runs ps_step(n_steps) between two CUDA events
+ * recorded on the simulation's stream and returns the device milliseconds.
+ * ps_profile_steps runs n_steps with every kernel launched on its own
+ * between events and returns, per kernel kind (PS_K_*), the summed device
+ * milliseconds and the launch count. */
+#define PS_K_BEGIN 0     /* integrate + container + hash + count (first step of a call) */
+#define PS_K_SCAN 1      /* decoupled look-back scan of the cell counts                  */
+#define PS_K_SCATTER 2   /* slot ids into cell order, count reset                        */
+#define PS_K_RANK_MOVE 3 /* canonical in-cell rank + state move                          */
+#define PS_K_CONTACTS 4  /* sphere contacts (+ next integrate/container/hash/count)      */
+#define PS_K_COUNT 5
+int ps_time_steps(ps_sim* sim, int64_t n_steps, double* device_ms);
+int ps_profile_steps(ps_sim* sim, int64_t n_steps, double* kernel_ms, int64_t* kernel_launches);
+
+int ps_destroy(ps_sim* sim);
+
+/* runSimulateCUDA with POD arguments: create, upload, max_steps steps,
+ * download, destroy.  aos_out may alias aos_in. */
+int ps_simulate(const ps_scene_desc* scene, const double* aos_in, double* aos_out, int64_t max_steps,
+                int32_t precision);
+
+/* Exclusive prefix sum of n uint32 on the device (PrefixScan::sum_scan_blelloch,
+ * src/ParticleStabilizerCUDA/PrefixScan.cu:232-268), single pass with
+ * decoupled look-back.  d_in may equal d_out.  d_scratch must hold
+ * ps_exclusive_scan_scratch_bytes(n) bytes; the call clears it.  Ordered on
+ * `stream` (a cudaStream_t, NULL = legacy default stream). */
+size_t ps_exclusive_scan_scratch_bytes(int64_t n);
+int ps_exclusive_scan_u32(const uint32_t* d_in, uint32_t* d_out, int64_t n, void* d_scratch, void* stream);
+
+/* CSV particle file, the reference's format (src/ParticleStabilizer/ParticleIO.cpp:58-144):
+ * header line skipped; rows x,y,z,r; mass = density*4/3*pi*r^3; velocity is
+ * the given vector.  ps_read_csv returns the row count in *n_out and fills
+ * at most `cap` rows.  ps_write_csv writes x,y,z,radius in fixed 10-char fields. */
+int ps_read_csv(const char* path, const double velocity[3], double density, double* aos_out, int64_t cap,
+                int64_t* n_out);
+int ps_write_csv(const char* path, const double* aos, int64_t n);
+
+/* OBJ container file (PolygonContainerCUDA::readFromFile,
+ * PolygonContainerCUDA.cpp:314-350): triangles de-indexed to 9 doubles each,
+ * vertices read in single precision as assimp's default ai_real. */
+int ps_read_obj(const char* path, double* tri_out, int64_t cap, int64_t* n_tri_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PARTICLE_STABILIZER_B200_H */

@@ -1,0 +1,106 @@
+// ps_device.cuh — device-side types and arithmetic shared by the step kernels.
+//
+// Every floating-point operation of the step is issued as one explicitly
+// rounded intrinsic (__fadd_rn, __fmaf_rn, ... / __dadd_rn, __fma_rn, ...),
+// which the compiler never contracts or reorders.  The operation sequence is
+// the one the CPU oracle (oracle/ps_oracle_impl.inc) performs, so results are
+// reproducible bit for bit in FP32 and in FP64.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace psb {
+
+// ---- explicit-rounding arithmetic -----------------------------------------
+template <class T>
+struct Ar;
+
+template <>
+struct Ar<float> {
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+  static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+  static __device__ __forceinline__ float sqrt(float a) { return __fsqrt_rn(a); }
+};
+
+template <>
+struct Ar<double> {
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+  static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+  static __device__ __forceinline__ double sqrt(double a) { return __dsqrt_rn(a); }
+};
+
+// ---- per-particle vector types ---------------------------------------------
+// pos_r = (x, y, z, radius), vel_m = (vx, vy, vz, mass): 32 B per particle in
+// FP32 (two float4), 64 B in FP64 (two double4, 32-byte aligned).
+template <class T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  using type = float4;
+};
+template <>
+struct Vec4<double> {
+  struct __align__(32) type {
+    double x, y, z, w;
+  };
+};
+template <class T>
+using vec4_t = typename Vec4<T>::type;
+
+template <class T>
+__device__ __forceinline__ vec4_t<T> ld4(const vec4_t<T>* p) {
+  return *p;
+}
+template <>
+__device__ __forceinline__ float4 ld4<float>(const float4* p) {
+  return __ldg(p);
+}
+
+// ---- per-scene parameters (device copy) -----------------------------------
+// Scenes are concatenated: scene s owns particle slots [pbase, pbase+pcount)
+// and cells [cbase, cbase + nb.x*nb.y*nb.z) of the global arrays.  The
+// canonical order sorts by global cell id, so a scene's particles never leave
+// its slot range.
+template <class T>
+struct SceneParams {
+  T grid_lo[3];   // grid domain minimum
+  T interval;     // cell edge
+  T box_lo[3];    // box walls
+  T box_hi[3];
+  T e_lo[3];      // restitution of the x/y/z min walls
+  T e_hi[3];      // restitution of the x/y/z max walls
+  T gravity[3];
+  T dt;
+  T k_spring;
+  T e_sphere;
+  T e_poly;       // triangle-container restitution
+  int32_t nb[3];  // cells per axis
+  uint32_t cbase; // first global cell id
+  uint32_t pbase; // first particle slot
+  uint32_t pcount;
+  // triangle container (mesh_tris == 0: box walls)
+  uint32_t mesh_tri_base;  // first triangle in the global soup
+  uint32_t mesh_tris;
+  uint32_t mesh_bin_base;  // first bin of this scene's triangle bins
+  int32_t mesh_nb[3];      // triangle-bin grid
+  T mesh_lo[3];            // triangle-bin grid origin
+  T mesh_iv;               // triangle-bin edge
+  int32_t edge_quirk;
+  int32_t pad_;
+};
+
+// Device error word bits (read by the host after a step block).
+enum : uint32_t {
+  PS_DEVERR_SCAN_TIMEOUT = 1u << 0,   // decoupled look-back gave up waiting
+  PS_DEVERR_MESH_OVERFLOW = 1u << 1,  // a particle hit more triangles than the hit buffer holds
+  PS_DEVERR_BAD_CELL = 1u << 2,       // a cell id fell outside its scene (never expected)
+};
+
+}  // namespace psb

@@ -1,0 +1,962 @@
+// ps_engine.cu — host engine and C ABI of libparticle_stabilizer_cuda.so.
+//
+// Owns the device state of one or many scenes, sizes their grids
+// (ParticleModelCUDA::initBuckets, src/ParticleStabilizerCUDA/ParticleModelCUDA.cpp:62-113),
+// bins container triangles, and issues blocks of steps as CUDA graphs on a
+// private stream.  The step sequence replaces the host loop of
+// PhysicsEngineCUDA::startSimulationLoop (PhysicsEngineCUDA.cpp:33-76), which
+// synchronises the device after every one of its 7+ launches per step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "particle_stabilizer_b200.h"
+#include "ps_scan.cuh"
+#include "ps_stats.cuh"
+#include "ps_step_kernels.cuh"
+
+using namespace psb;
+
+// ---- error reporting ---------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define PS_CUDA(expr)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (expr);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(e_ == cudaErrorMemoryAllocation ? PS_ERR_NOMEM : PS_ERR_CUDA,             \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));                      \
+  } while (0)
+
+extern "C" const char* ps_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int ps_internal_fail(int code, const char* msg) { return fail(code, msg ? msg : ""); }
+
+namespace {
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && cudaSetDevice(dev) == cudaSuccess) ok = true;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+struct GridHost {
+  double min[3], max[3], interval;
+  int32_t nb[3];
+  int64_t n_cells, cbase;
+  // triangle bins
+  double mesh_lo[3], mesh_iv;
+  int32_t mesh_nb[3];
+  int64_t n_bins, bin_base, tri_base, n_tri;
+};
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+struct ps_sim {
+  int precision = PS_FP32;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int n_scenes = 0;
+  std::vector<ps_scene_desc> desc;
+  std::vector<std::vector<double>> tris;  // owned copies of the triangle soups
+  std::vector<int64_t> pbase;             // n_scenes + 1
+  int64_t n_total = 0;
+  bool multi = false, has_mesh = false;
+
+  // grids (sized on the first ps_set_state)
+  bool grid_sized = false, grid_valid = false, stepped = false;
+  std::vector<GridHost> grids;
+  int64_t c_total = 0, bins_total = 0, tri_total = 0;
+
+  // device memory
+  void* part_arena = nullptr;
+  void* cell_arena = nullptr;
+  void *P0 = nullptr, *V0 = nullptr, *P1 = nullptr, *V1 = nullptr;
+  uint32_t *orig = nullptr, *cell = nullptr, *slot = nullptr, *tmp = nullptr;
+  uint32_t *count = nullptr, *offset = nullptr, *err = nullptr, *d_pbase = nullptr;
+  uint64_t* scan_scratch = nullptr;
+  double* staging = nullptr;  // n_total x 8 doubles
+  void* d_scenes = nullptr;
+  StatsPartial* d_stats = nullptr;
+  StatsPartial* d_stats_out = nullptr;
+  // triangle data
+  void *d_tri = nullptr, *d_nrm = nullptr, *d_aabb = nullptr;
+  uint32_t *d_bin_offset = nullptr, *d_bin_tri = nullptr;
+  MeshView* d_mesh_view = nullptr;
+
+  std::vector<SceneParams<float>> sp32;
+  std::vector<SceneParams<double>> sp64;
+
+  std::map<int64_t, cudaGraphExec_t> graphs;
+  int64_t last_launches = 0;
+  std::map<int32_t, void*> checkpoints;  // slot -> device copy of (P0, V1, orig)
+};
+
+namespace {
+
+constexpr int64_t kGraphBlock = 200;  // steps per captured graph
+
+int64_t n_scan(const ps_sim* s) { return s->c_total + 1; }
+uint32_t scan_words(const ps_sim* s) { return (uint32_t)(scan_num_tiles(n_scan(s)) + 1); }
+
+template <class T>
+StepBufs<T> bufs(ps_sim* s) {
+  StepBufs<T> b;
+  b.P0 = static_cast<vec4_t<T>*>(s->P0);
+  b.V0 = static_cast<vec4_t<T>*>(s->V0);
+  b.P1 = static_cast<vec4_t<T>*>(s->P1);
+  b.V1 = static_cast<vec4_t<T>*>(s->V1);
+  b.orig = s->orig;
+  b.cell = s->cell;
+  b.slot = s->slot;
+  b.tmp = s->tmp;
+  b.count = s->count;
+  b.offset = s->offset;
+  b.err = s->err;
+  b.scenes = static_cast<const SceneParams<T>*>(s->d_scenes);
+  b.pbase = s->d_pbase;
+  b.n_scenes = s->n_scenes;
+  b.n = (uint32_t)s->n_total;
+  b.scan_scratch = s->scan_scratch;
+  b.scan_words = scan_words(s);
+  return b;
+}
+
+template <class T>
+const std::vector<SceneParams<T>>& params(const ps_sim* s);
+template <>
+const std::vector<SceneParams<float>>& params<float>(const ps_sim* s) {
+  return s->sp32;
+}
+template <>
+const std::vector<SceneParams<double>>& params<double>(const ps_sim* s) {
+  return s->sp64;
+}
+
+unsigned blocks_for(int64_t n) { return (unsigned)((n + STEP_THREADS - 1) / STEP_THREADS); }
+
+// ---- the launch sequence -----------------------------------------------------
+template <class T, bool MULTI, bool MESH>
+int64_t enqueue_steps(ps_sim* s, int64_t steps) {
+  const StepBufs<T> b = bufs<T>(s);
+  const SceneParams<T> sp0 = params<T>(s)[0];
+  const unsigned gb = blocks_for(std::max<int64_t>(s->n_total, scan_words(s)));
+  const unsigned gp = blocks_for(s->n_total);
+  const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
+  cudaStream_t st = s->stream;
+  int64_t launches = 0;
+  k_begin<T, MULTI, MESH, true><<<gb, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+  ++launches;
+  for (int64_t k = 0; k < steps; ++k) {
+    k_exclusive_scan_u32<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->scan_scratch, s->err);
+    k_scatter<<<gb, STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp, s->count,
+                                           (uint32_t)s->n_total, s->scan_scratch, scan_words(s));
+    k_rank_move<T><<<gp, STEP_THREADS, 0, st>>>(b);
+    if (k + 1 < steps)
+      k_contacts<T, MULTI, MESH, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+    else
+      k_contacts<T, MULTI, MESH, false><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+    launches += 4;
+  }
+  return launches;
+}
+
+// Eager launch sequence with an event pair around every kernel (profiling).
+struct LaunchRecord {
+  int kind;
+  cudaEvent_t a, b;
+};
+
+template <class T, bool MULTI, bool MESH>
+void enqueue_steps_recorded(ps_sim* s, int64_t steps, std::vector<LaunchRecord>& rec) {
+  const StepBufs<T> b = bufs<T>(s);
+  const SceneParams<T> sp0 = params<T>(s)[0];
+  const unsigned gb = blocks_for(std::max<int64_t>(s->n_total, scan_words(s)));
+  const unsigned gp = blocks_for(s->n_total);
+  const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
+  cudaStream_t st = s->stream;
+  size_t r = 0;
+  auto pre = [&](int kind) {
+    rec[r].kind = kind;
+    cudaEventRecord(rec[r].a, st);
+  };
+  auto post = [&]() { cudaEventRecord(rec[r++].b, st); };
+  pre(PS_K_BEGIN);
+  k_begin<T, MULTI, MESH, true><<<gb, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+  post();
+  for (int64_t k = 0; k < steps; ++k) {
+    pre(PS_K_SCAN);
+    k_exclusive_scan_u32<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->scan_scratch, s->err);
+    post();
+    pre(PS_K_SCATTER);
+    k_scatter<<<gb, STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp, s->count,
+                                           (uint32_t)s->n_total, s->scan_scratch, scan_words(s));
+    post();
+    pre(PS_K_RANK_MOVE);
+    k_rank_move<T><<<gp, STEP_THREADS, 0, st>>>(b);
+    post();
+    pre(PS_K_CONTACTS);
+    if (k + 1 < steps)
+      k_contacts<T, MULTI, MESH, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+    else
+      k_contacts<T, MULTI, MESH, false><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+    post();
+  }
+}
+
+template <class T>
+void enqueue_steps_recorded_dispatch(ps_sim* s, int64_t steps, std::vector<LaunchRecord>& rec) {
+  if (s->multi) {
+    if (s->has_mesh)
+      enqueue_steps_recorded<T, true, true>(s, steps, rec);
+    else
+      enqueue_steps_recorded<T, true, false>(s, steps, rec);
+  } else {
+    if (s->has_mesh)
+      enqueue_steps_recorded<T, false, true>(s, steps, rec);
+    else
+      enqueue_steps_recorded<T, false, false>(s, steps, rec);
+  }
+}
+
+template <class T>
+int64_t enqueue_steps_dispatch(ps_sim* s, int64_t steps) {
+  if (s->multi) {
+    return s->has_mesh ? enqueue_steps<T, true, true>(s, steps) : enqueue_steps<T, true, false>(s, steps);
+  }
+  return s->has_mesh ? enqueue_steps<T, false, true>(s, steps) : enqueue_steps<T, false, false>(s, steps);
+}
+
+// Rebuild the grid of the at-rest state without moving it (statistics and
+// bucket queries before the first step).
+template <class T, bool MULTI>
+void enqueue_regrid(ps_sim* s) {
+  const StepBufs<T> b = bufs<T>(s);
+  const SceneParams<T> sp0 = params<T>(s)[0];
+  const unsigned gb = blocks_for(std::max<int64_t>(s->n_total, scan_words(s)));
+  const unsigned gp = blocks_for(s->n_total);
+  cudaStream_t st = s->stream;
+  k_begin<T, MULTI, false, false><<<gb, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+  k_exclusive_scan_u32<<<(unsigned)scan_num_tiles(n_scan(s)), SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s),
+                                                                                    s->scan_scratch, s->err);
+  k_scatter<<<gb, STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp, s->count,
+                                         (uint32_t)s->n_total, s->scan_scratch, scan_words(s));
+  k_rank_move<T><<<gp, STEP_THREADS, 0, st>>>(b);
+  k_copy_vel<T><<<gp, STEP_THREADS, 0, st>>>(b);
+}
+
+int regrid(ps_sim* s) {
+  if (s->n_total == 0) {
+    s->grid_valid = true;
+    return PS_OK;
+  }
+  if (s->precision == PS_FP32)
+    s->multi ? enqueue_regrid<float, true>(s) : enqueue_regrid<float, false>(s);
+  else
+    s->multi ? enqueue_regrid<double, true>(s) : enqueue_regrid<double, false>(s);
+  PS_CUDA(cudaGetLastError());
+  s->grid_valid = true;
+  return PS_OK;
+}
+
+int check_device_error(ps_sim* s) {
+  uint32_t e = 0;
+  PS_CUDA(cudaMemcpyAsync(&e, s->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+  PS_CUDA(cudaStreamSynchronize(s->stream));
+  if (e != 0) {
+    std::string m = "device error word 0x" + std::to_string(e) + ":";
+    if (e & PS_DEVERR_SCAN_TIMEOUT) m += " scan look-back wait expired;";
+    if (e & PS_DEVERR_MESH_OVERFLOW) m += " a particle hit more than 64 triangles in one step;";
+    if (e & PS_DEVERR_BAD_CELL) m += " cell id outside its scene;";
+    uint32_t zero = 0;
+    cudaMemcpyAsync(s->err, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream);
+    cudaStreamSynchronize(s->stream);
+    return fail(PS_ERR_DEVICE, m);
+  }
+  return PS_OK;
+}
+
+// ---- conversion kernels between the host AoS and the device SoA ------------
+template <class T>
+__global__ void k_upload(const double* __restrict__ aos, vec4_t<T>* P0, vec4_t<T>* V1, uint32_t* orig, uint32_t n) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double* q = aos + 8 * (size_t)p;
+  vec4_t<T> P, V;
+  P.x = (T)q[0];
+  P.y = (T)q[1];
+  P.z = (T)q[2];
+  P.w = (T)q[6];
+  V.x = (T)q[3];
+  V.y = (T)q[4];
+  V.z = (T)q[5];
+  V.w = (T)q[7];
+  P0[p] = P;
+  V1[p] = V;
+  orig[p] = p;
+}
+
+template <class T>
+__global__ void k_download(double* __restrict__ aos, const vec4_t<T>* P0, const vec4_t<T>* V1, const uint32_t* orig,
+                           uint32_t n) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const vec4_t<T> P = P0[p], V = V1[p];
+  double* q = aos + 8 * (size_t)orig[p];
+  q[0] = (double)P.x;
+  q[1] = (double)P.y;
+  q[2] = (double)P.z;
+  q[3] = (double)V.x;
+  q[4] = (double)V.y;
+  q[5] = (double)V.z;
+  q[6] = (double)P.w;
+  q[7] = (double)V.w;
+}
+
+__global__ void k_counts_from_offsets(const uint32_t* offset, uint32_t* counts, int64_t n) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) counts[c] = offset[c + 1] - offset[c];
+}
+
+// ---- set-up ------------------------------------------------------------------
+template <class T>
+SceneParams<T> make_params(const ps_scene_desc& d, const GridHost& g, int64_t pbase, int64_t pcount) {
+  SceneParams<T> sp{};
+  for (int a = 0; a < 3; ++a) {
+    sp.grid_lo[a] = (T)g.min[a];
+    sp.box_lo[a] = (T)d.box_min[a];
+    sp.box_hi[a] = (T)d.box_max[a];
+    sp.gravity[a] = (T)d.gravity[a];
+    sp.nb[a] = g.nb[a];
+    sp.mesh_nb[a] = g.mesh_nb[a];
+    sp.mesh_lo[a] = (T)g.mesh_lo[a];
+  }
+  sp.interval = (T)g.interval;
+  sp.e_lo[0] = (T)d.e_wall[PS_XMIN];
+  sp.e_lo[1] = (T)d.e_wall[PS_YMIN];
+  sp.e_lo[2] = (T)d.e_wall[PS_ZMIN];
+  sp.e_hi[0] = (T)d.e_wall[PS_XMAX];
+  sp.e_hi[1] = (T)d.e_wall[PS_YMAX];
+  sp.e_hi[2] = (T)d.e_wall[PS_ZMAX];
+  sp.dt = (T)d.dt;
+  sp.k_spring = (T)d.k_spring;
+  sp.e_sphere = (T)d.e_sphere;
+  sp.e_poly = (T)d.e_wall[PS_ZMIN];  // polygon restitution = zMin (PhysicsEngineCUDA.cpp:112-114)
+  sp.cbase = (uint32_t)g.cbase;
+  sp.pbase = (uint32_t)pbase;
+  sp.pcount = (uint32_t)pcount;
+  sp.mesh_tri_base = (uint32_t)g.tri_base;
+  sp.mesh_tris = (uint32_t)g.n_tri;
+  sp.mesh_bin_base = (uint32_t)g.bin_base;
+  sp.mesh_iv = (T)g.mesh_iv;
+  sp.edge_quirk = d.edge_quirk;
+  return sp;
+}
+
+// Host copy of the device bin function (same float/double operations).
+template <class T>
+int32_t host_mesh_axis(T x, T lo, T iv, int32_t nb) {
+  const T q = (x - lo) / iv;
+  if (!(q > T(0))) return 0;
+  if (q >= (T)nb) return nb - 1;
+  return (int32_t)q;
+}
+
+// Triangle data in precision T for every scene, binned by AABB.
+template <class T>
+int upload_mesh(ps_sim* s) {
+  std::vector<T> tri, nrm, aabb;
+  std::vector<uint32_t> bin_offset((size_t)s->bins_total + 1, 0), bin_tri;
+  std::vector<std::vector<uint32_t>> per_bin_counts;
+  tri.reserve((size_t)s->tri_total * 9);
+  for (int sc = 0; sc < s->n_scenes; ++sc) {
+    const GridHost& g = s->grids[sc];
+    const std::vector<double>& soup = s->tris[sc];
+    for (int64_t t = 0; t < g.n_tri; ++t) {
+      const double* v = soup.data() + 9 * t;
+      for (int k = 0; k < 9; ++k) tri.push_back((T)v[k]);
+      // unit normal as PolygonContainerCUDA.cpp:73-88 (double, component / length)
+      const double r0x = v[3] - v[0], r0y = v[4] - v[1], r0z = v[5] - v[2];
+      const double r1x = v[6] - v[0], r1y = v[7] - v[1], r1z = v[8] - v[2];
+      const double nx = r0y * r1z - r0z * r1y, ny = r0z * r1x - r0x * r1z, nz = r0x * r1y - r0y * r1x;
+      const double len = std::sqrt(nx * nx + ny * ny + nz * nz);
+      nrm.push_back((T)(nx / len));
+      nrm.push_back((T)(ny / len));
+      nrm.push_back((T)(nz / len));
+      for (int a = 0; a < 3; ++a) aabb.push_back(std::min(std::min((T)v[a], (T)v[3 + a]), (T)v[6 + a]));
+      for (int a = 0; a < 3; ++a) aabb.push_back(std::max(std::max((T)v[a], (T)v[3 + a]), (T)v[6 + a]));
+    }
+  }
+  // two passes: count, then fill (ascending triangle id inside each bin)
+  for (int pass = 0; pass < 2; ++pass) {
+    std::vector<uint32_t> fill;
+    if (pass == 1) {
+      for (int64_t i = 0; i < s->bins_total; ++i) bin_offset[i + 1] += bin_offset[i];
+      bin_tri.resize(bin_offset[s->bins_total]);
+      fill.assign(bin_offset.begin(), bin_offset.end() - 1);
+    }
+    for (int sc = 0; sc < s->n_scenes; ++sc) {
+      const GridHost& g = s->grids[sc];
+      const T lo[3] = {(T)g.mesh_lo[0], (T)g.mesh_lo[1], (T)g.mesh_lo[2]};
+      const T iv = (T)g.mesh_iv;
+      for (int64_t t = 0; t < g.n_tri; ++t) {
+        const int64_t gt = g.tri_base + t;
+        int32_t b0[3], b1[3];
+        for (int a = 0; a < 3; ++a) {
+          b0[a] = host_mesh_axis<T>(aabb[6 * gt + a], lo[a], iv, g.mesh_nb[a]);
+          b1[a] = host_mesh_axis<T>(aabb[6 * gt + 3 + a], lo[a], iv, g.mesh_nb[a]);
+        }
+        for (int32_t x = b0[0]; x <= b1[0]; ++x)
+          for (int32_t y = b0[1]; y <= b1[1]; ++y)
+            for (int32_t z = b0[2]; z <= b1[2]; ++z) {
+              const int64_t bin = g.bin_base + ((int64_t)x * g.mesh_nb[1] + y) * g.mesh_nb[2] + z;
+              if (pass == 0)
+                bin_offset[bin + 1] += 1;
+              else
+                bin_tri[fill[bin]++] = (uint32_t)gt;
+            }
+      }
+    }
+  }
+  const size_t bt = tri.size() * sizeof(T), bn = nrm.size() * sizeof(T), ba = aabb.size() * sizeof(T);
+  PS_CUDA(cudaMalloc(&s->d_tri, std::max<size_t>(bt, 16)));
+  PS_CUDA(cudaMalloc(&s->d_nrm, std::max<size_t>(bn, 16)));
+  PS_CUDA(cudaMalloc(&s->d_aabb, std::max<size_t>(ba, 16)));
+  PS_CUDA(cudaMalloc(&s->d_bin_offset, bin_offset.size() * sizeof(uint32_t)));
+  PS_CUDA(cudaMalloc(&s->d_bin_tri, std::max<size_t>(bin_tri.size(), 1) * sizeof(uint32_t)));
+  PS_CUDA(cudaMalloc(&s->d_mesh_view, sizeof(MeshView)));
+  PS_CUDA(cudaMemcpy(s->d_tri, tri.data(), bt, cudaMemcpyHostToDevice));
+  PS_CUDA(cudaMemcpy(s->d_nrm, nrm.data(), bn, cudaMemcpyHostToDevice));
+  PS_CUDA(cudaMemcpy(s->d_aabb, aabb.data(), ba, cudaMemcpyHostToDevice));
+  PS_CUDA(cudaMemcpy(s->d_bin_offset, bin_offset.data(), bin_offset.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  if (!bin_tri.empty())
+    PS_CUDA(cudaMemcpy(s->d_bin_tri, bin_tri.data(), bin_tri.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  const MeshView mv{s->d_tri, s->d_nrm, s->d_aabb, s->d_bin_offset, s->d_bin_tri};
+  PS_CUDA(cudaMemcpy(s->d_mesh_view, &mv, sizeof(MeshView), cudaMemcpyHostToDevice));
+  return PS_OK;
+}
+
+// Size every scene's grid from its radii and allocate the per-cell arrays.
+int size_grids(ps_sim* s, const double* aos) {
+  s->grids.assign(s->n_scenes, GridHost{});
+  int64_t cbase = 0, bin_base = 0, tri_base = 0;
+  for (int sc = 0; sc < s->n_scenes; ++sc) {
+    const ps_scene_desc& d = s->desc[sc];
+    GridHost& g = s->grids[sc];
+    double r_max = 0.0;
+    double plo[3] = {INFINITY, INFINITY, INFINITY}, phi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = s->pbase[sc]; i < s->pbase[sc + 1]; ++i) {
+      const double* q = aos + 8 * i;
+      if (!(q[6] >= 0.0) || !std::isfinite(q[6]) || !(q[7] > 0.0))
+        return fail(PS_ERR_INVALID, "scene " + std::to_string(sc) + ": particle " + std::to_string(i) +
+                                        " has a negative/non-finite radius or a non-positive mass");
+      r_max = std::max(r_max, q[6]);
+      for (int a = 0; a < 3; ++a) {
+        plo[a] = std::min(plo[a], q[a]);
+        phi[a] = std::max(phi[a], q[a]);
+      }
+    }
+    if (d.tri != nullptr && d.n_tri > 0) {
+      const std::vector<double>& soup = s->tris[sc];
+      for (int a = 0; a < 3; ++a) {
+        g.min[a] = INFINITY;
+        g.max[a] = -INFINITY;
+      }
+      for (int64_t k = 0; k < 3 * d.n_tri; ++k)
+        for (int a = 0; a < 3; ++a) {
+          g.min[a] = std::min(g.min[a], soup[3 * k + a]);
+          g.max[a] = std::max(g.max[a], soup[3 * k + a]);
+        }
+      for (int a = 0; a < 3; ++a) {
+        g.mesh_lo[a] = g.min[a];
+      }
+      double ext = 0.0;
+      for (int a = 0; a < 3; ++a) ext = std::max(ext, g.max[a] - g.min[a]);
+      if (d.widen_domain && s->pbase[sc + 1] > s->pbase[sc]) {
+        for (int a = 0; a < 3; ++a) {
+          g.min[a] = std::min(g.min[a], plo[a] - r_max);
+          g.max[a] = std::max(g.max[a], phi[a] + r_max);
+        }
+      }
+      g.n_tri = d.n_tri;
+      g.tri_base = tri_base;
+      tri_base += d.n_tri;
+      // bin edge: at least one particle cell, at most 128 bins along the longest side
+      g.mesh_iv = std::max(r_max * 2.0 * 1.05, ext / 128.0);
+      if (!(g.mesh_iv > 0.0)) g.mesh_iv = 1.0;
+      for (int a = 0; a < 3; ++a) {
+        double span = 0.0;
+        for (int64_t k = 0; k < 3 * d.n_tri; ++k) span = std::max(span, soup[3 * k + a] - g.mesh_lo[a]);
+        g.mesh_nb[a] = (int32_t)(span / g.mesh_iv) + 1;
+      }
+      g.n_bins = (int64_t)g.mesh_nb[0] * g.mesh_nb[1] * g.mesh_nb[2];
+      g.bin_base = bin_base;
+      bin_base += g.n_bins;
+    } else {
+      for (int a = 0; a < 3; ++a) {
+        g.min[a] = d.box_min[a];
+        g.max[a] = d.box_max[a];
+        g.mesh_nb[a] = 1;
+        g.mesh_lo[a] = 0.0;
+      }
+      g.mesh_iv = 1.0;
+    }
+    if (!(r_max > 0.0) && s->pbase[sc + 1] > s->pbase[sc])
+      return fail(PS_ERR_INVALID, "scene " + std::to_string(sc) + ": the largest radius must be positive");
+    g.interval = d.cell_size > 0.0 ? d.cell_size : r_max * 2.0 * 1.05;  // ParticleModelCUDA.cpp:84
+    if (!(g.interval > 0.0)) g.interval = 1.0;  // empty scene
+    if (g.interval < 2.0 * r_max)
+      return fail(PS_ERR_INVALID, "scene " + std::to_string(sc) + ": cell_size " + std::to_string(g.interval) +
+                                      " is smaller than 2*r_max = " + std::to_string(2.0 * r_max));
+    int64_t nc = 1;
+    for (int a = 0; a < 3; ++a) {
+      const double ncells = (g.max[a] - g.min[a]) / g.interval;
+      if (!(ncells >= 0.0) || ncells > 2.0e9)
+        return fail(PS_ERR_INVALID, "scene " + std::to_string(sc) + ": bad grid extent on axis " + std::to_string(a));
+      g.nb[a] = (int32_t)ncells + 1;  // ParticleModelCUDA.cpp:89-91
+      nc *= g.nb[a];
+    }
+    g.n_cells = nc;
+    g.cbase = cbase;
+    cbase += nc;
+    if (cbase >= (int64_t)UINT32_MAX - 1)
+      return fail(PS_ERR_INVALID, "too many grid cells over all scenes: " + std::to_string(cbase));
+  }
+  s->c_total = cbase;
+  s->bins_total = bin_base;
+  s->tri_total = tri_base;
+
+  // per-cell arrays and scan scratch
+  const size_t cells_b = align_up(sizeof(uint32_t) * (size_t)(s->c_total + 1), 256);
+  const size_t scratch_b = align_up(scan_scratch_bytes(n_scan(s)), 256);
+  PS_CUDA(cudaMalloc(&s->cell_arena, 2 * cells_b + scratch_b));
+  char* c = static_cast<char*>(s->cell_arena);
+  s->count = reinterpret_cast<uint32_t*>(c);
+  s->offset = reinterpret_cast<uint32_t*>(c + cells_b);
+  s->scan_scratch = reinterpret_cast<uint64_t*>(c + 2 * cells_b);
+  PS_CUDA(cudaMemset(s->count, 0, cells_b));
+  PS_CUDA(cudaMemset(s->offset, 0, cells_b));
+  PS_CUDA(cudaMemset(s->scan_scratch, 0, scratch_b));
+
+  // scene parameter tables
+  s->sp32.clear();
+  s->sp64.clear();
+  for (int sc = 0; sc < s->n_scenes; ++sc) {
+    const int64_t pc = s->pbase[sc + 1] - s->pbase[sc];
+    s->sp32.push_back(make_params<float>(s->desc[sc], s->grids[sc], s->pbase[sc], pc));
+    s->sp64.push_back(make_params<double>(s->desc[sc], s->grids[sc], s->pbase[sc], pc));
+  }
+  const size_t spb = s->precision == PS_FP32 ? sizeof(SceneParams<float>) : sizeof(SceneParams<double>);
+  PS_CUDA(cudaMalloc(&s->d_scenes, spb * s->n_scenes));
+  if (s->precision == PS_FP32)
+    PS_CUDA(cudaMemcpy(s->d_scenes, s->sp32.data(), spb * s->n_scenes, cudaMemcpyHostToDevice));
+  else
+    PS_CUDA(cudaMemcpy(s->d_scenes, s->sp64.data(), spb * s->n_scenes, cudaMemcpyHostToDevice));
+  if (s->has_mesh) {
+    const int rc = s->precision == PS_FP32 ? upload_mesh<float>(s) : upload_mesh<double>(s);
+    if (rc != PS_OK) return rc;
+  }
+  s->grid_sized = true;
+  return PS_OK;
+}
+
+void free_sim(ps_sim* s) {
+  for (auto& kv : s->checkpoints) cudaFree(kv.second);
+  s->checkpoints.clear();
+  for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+  cudaFree(s->part_arena);
+  cudaFree(s->cell_arena);
+  cudaFree(s->d_scenes);
+  cudaFree(s->d_tri);
+  cudaFree(s->d_nrm);
+  cudaFree(s->d_aabb);
+  cudaFree(s->d_bin_offset);
+  cudaFree(s->d_bin_tri);
+  cudaFree(s->d_mesh_view);
+  if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+}  // namespace
+
+// ---- C ABI -------------------------------------------------------------------
+extern "C" int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t precision, int32_t device,
+                         ps_sim** out) {
+  if (out == nullptr || scenes == nullptr || n_scenes <= 0)
+    return fail(PS_ERR_INVALID, "ps_create: scenes, n_scenes > 0 and out are required");
+  *out = nullptr;
+  if (precision != PS_FP32 && precision != PS_FP64) return fail(PS_ERR_INVALID, "ps_create: precision must be PS_FP32 or PS_FP64");
+  int ndev = 0;
+  PS_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(PS_ERR_INVALID, "ps_create: no CUDA device " + std::to_string(device));
+  DeviceGuard guard(device);
+  if (!guard.ok) return fail(PS_ERR_CUDA, "ps_create: cannot select device " + std::to_string(device));
+
+  ps_sim* s = new ps_sim();
+  s->precision = precision;
+  s->device = device;
+  s->n_scenes = n_scenes;
+  s->desc.assign(scenes, scenes + n_scenes);
+  s->tris.resize(n_scenes);
+  s->pbase.assign(n_scenes + 1, 0);
+  for (int sc = 0; sc < n_scenes; ++sc) {
+    const ps_scene_desc& d = scenes[sc];
+    if (d.n_particles < 0 || !(d.dt >= 0.0) || (d.tri == nullptr && d.n_tri != 0) || d.n_tri < 0) {
+      delete s;
+      return fail(PS_ERR_INVALID, "ps_create: scene " + std::to_string(sc) + " has a negative count, a bad dt or an inconsistent triangle list");
+    }
+    if (d.tri != nullptr && d.n_tri > 0) {
+      s->tris[sc].assign(d.tri, d.tri + 9 * d.n_tri);
+      s->has_mesh = true;
+    }
+    s->desc[sc].tri = nullptr;  // owned copy lives in s->tris
+    s->pbase[sc + 1] = s->pbase[sc] + d.n_particles;
+  }
+  s->n_total = s->pbase[n_scenes];
+  s->multi = n_scenes > 1;
+  if (s->n_total >= (int64_t)UINT32_MAX - 1) {
+    delete s;
+    return fail(PS_ERR_INVALID, "ps_create: too many particles");
+  }
+  const size_t vb = s->precision == PS_FP32 ? 16 : 32;
+  const size_t n = (size_t)std::max<int64_t>(s->n_total, 1);
+  const size_t b4 = align_up(vb * n, 256), bu = align_up(4 * n, 256), bs = align_up(64 * n, 256);
+  const size_t bp = align_up(4 * (size_t)(n_scenes + 1), 256);
+  cudaError_t e = cudaMalloc(&s->part_arena, 4 * b4 + 4 * bu + bs + 256 + bp + 2 * sizeof(StatsPartial) * kStatsBlocks + 256);
+  if (e != cudaSuccess) {
+    delete s;
+    return fail(e == cudaErrorMemoryAllocation ? PS_ERR_NOMEM : PS_ERR_CUDA, std::string("ps_create: ") + cudaGetErrorString(e));
+  }
+  char* p = static_cast<char*>(s->part_arena);
+  s->P0 = p; p += b4;
+  s->V0 = p; p += b4;
+  s->P1 = p; p += b4;
+  s->V1 = p; p += b4;
+  s->orig = reinterpret_cast<uint32_t*>(p); p += bu;
+  s->cell = reinterpret_cast<uint32_t*>(p); p += bu;
+  s->slot = reinterpret_cast<uint32_t*>(p); p += bu;
+  s->tmp = reinterpret_cast<uint32_t*>(p); p += bu;
+  s->staging = reinterpret_cast<double*>(p); p += bs;
+  s->err = reinterpret_cast<uint32_t*>(p); p += 256;
+  s->d_pbase = reinterpret_cast<uint32_t*>(p); p += bp;
+  s->d_stats = reinterpret_cast<StatsPartial*>(p); p += sizeof(StatsPartial) * kStatsBlocks;
+  s->d_stats_out = reinterpret_cast<StatsPartial*>(p);
+  std::vector<uint32_t> pb(n_scenes + 1);
+  for (int sc = 0; sc <= n_scenes; ++sc) pb[sc] = (uint32_t)s->pbase[sc];
+  e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMemcpy(s->d_pbase, pb.data(), 4 * pb.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(s->err, 0, 256);
+  if (e != cudaSuccess) {
+    free_sim(s);
+    delete s;
+    return fail(PS_ERR_CUDA, std::string("ps_create: ") + cudaGetErrorString(e));
+  }
+  *out = s;
+  return PS_OK;
+}
+
+extern "C" int ps_set_state(ps_sim* s, const double* aos, int64_t n_total) {
+  if (s == nullptr || (aos == nullptr && n_total > 0)) return fail(PS_ERR_INVALID, "ps_set_state: null argument");
+  if (n_total != s->n_total)
+    return fail(PS_ERR_INVALID, "ps_set_state: expected " + std::to_string(s->n_total) + " particles, got " + std::to_string(n_total));
+  DeviceGuard guard(s->device);
+  if (!s->grid_sized) {
+    const int rc = size_grids(s, aos);
+    if (rc != PS_OK) return rc;
+  } else {
+    for (int sc = 0; sc < s->n_scenes; ++sc)
+      for (int64_t i = s->pbase[sc]; i < s->pbase[sc + 1]; ++i)
+        if (!(2.0 * aos[8 * i + 6] <= s->grids[sc].interval) || !(aos[8 * i + 7] > 0.0))
+          return fail(PS_ERR_INVALID, "ps_set_state: particle " + std::to_string(i) + " does not fit the grid sized by the first upload");
+  }
+  if (n_total == 0) return PS_OK;
+  PS_CUDA(cudaMemcpyAsync(s->staging, aos, 64 * (size_t)n_total, cudaMemcpyHostToDevice, s->stream));
+  const unsigned g = blocks_for(n_total);
+  if (s->precision == PS_FP32)
+    k_upload<float><<<g, STEP_THREADS, 0, s->stream>>>(s->staging, static_cast<float4*>(s->P0),
+                                                       static_cast<float4*>(s->V1), s->orig, (uint32_t)n_total);
+  else
+    k_upload<double><<<g, STEP_THREADS, 0, s->stream>>>(s->staging, static_cast<vec4_t<double>*>(s->P0),
+                                                        static_cast<vec4_t<double>*>(s->V1), s->orig, (uint32_t)n_total);
+  PS_CUDA(cudaGetLastError());
+  PS_CUDA(cudaStreamSynchronize(s->stream));
+  s->grid_valid = false;
+  return PS_OK;
+}
+
+extern "C" int ps_get_state(ps_sim* s, double* out, int64_t n_total) {
+  if (s == nullptr || (out == nullptr && n_total > 0)) return fail(PS_ERR_INVALID, "ps_get_state: null argument");
+  if (n_total != s->n_total) return fail(PS_ERR_INVALID, "ps_get_state: size mismatch");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_get_state: no state uploaded");
+  if (n_total == 0) return PS_OK;
+  DeviceGuard guard(s->device);
+  const unsigned g = blocks_for(n_total);
+  if (s->precision == PS_FP32)
+    k_download<float><<<g, STEP_THREADS, 0, s->stream>>>(s->staging, static_cast<float4*>(s->P0),
+                                                         static_cast<float4*>(s->V1), s->orig, (uint32_t)n_total);
+  else
+    k_download<double><<<g, STEP_THREADS, 0, s->stream>>>(s->staging, static_cast<vec4_t<double>*>(s->P0),
+                                                          static_cast<vec4_t<double>*>(s->V1), s->orig, (uint32_t)n_total);
+  PS_CUDA(cudaGetLastError());
+  PS_CUDA(cudaMemcpyAsync(out, s->staging, 64 * (size_t)n_total, cudaMemcpyDeviceToHost, s->stream));
+  PS_CUDA(cudaStreamSynchronize(s->stream));
+  return check_device_error(s);
+}
+
+extern "C" int ps_step(ps_sim* s, int64_t n_steps) {
+  if (s == nullptr || n_steps < 0) return fail(PS_ERR_INVALID, "ps_step: bad argument");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_step: call ps_set_state first");
+  s->last_launches = 0;
+  if (n_steps == 0 || s->n_total == 0) return PS_OK;
+  DeviceGuard guard(s->device);
+  int64_t left = n_steps;
+  while (left > 0) {
+    const int64_t L = std::min(left, kGraphBlock);
+    auto it = s->graphs.find(L);
+    if (it == s->graphs.end()) {
+      cudaGraph_t graph = nullptr;
+      PS_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+      const int64_t nl = s->precision == PS_FP32 ? enqueue_steps_dispatch<float>(s, L) : enqueue_steps_dispatch<double>(s, L);
+      (void)nl;
+      const cudaError_t ce = cudaGetLastError();
+      const cudaError_t ee = cudaStreamEndCapture(s->stream, &graph);
+      if (ce != cudaSuccess || ee != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(PS_ERR_CUDA, std::string("ps_step: capture failed: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+      }
+      cudaGraphExec_t exec = nullptr;
+      const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) return fail(PS_ERR_CUDA, std::string("ps_step: instantiate failed: ") + cudaGetErrorString(ie));
+      it = s->graphs.emplace(L, exec).first;
+    }
+    PS_CUDA(cudaGraphLaunch(it->second, s->stream));
+    s->last_launches += 1 + 4 * L;
+    left -= L;
+  }
+  s->grid_valid = true;
+  s->stepped = true;
+  return PS_OK;
+}
+
+extern "C" int ps_checkpoint_save(ps_sim* s, int32_t slot) {
+  if (s == nullptr || slot < 0) return fail(PS_ERR_INVALID, "ps_checkpoint_save: bad argument");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_checkpoint_save: no state uploaded");
+  DeviceGuard guard(s->device);
+  const size_t vb = (s->precision == PS_FP32 ? 16 : 32) * (size_t)s->n_total, ob = 4 * (size_t)s->n_total;
+  void*& buf = s->checkpoints[slot];
+  if (buf == nullptr) PS_CUDA(cudaMalloc(&buf, std::max<size_t>(2 * vb + ob, 16)));
+  char* p = static_cast<char*>(buf);
+  PS_CUDA(cudaMemcpyAsync(p, s->P0, vb, cudaMemcpyDeviceToDevice, s->stream));
+  PS_CUDA(cudaMemcpyAsync(p + vb, s->V1, vb, cudaMemcpyDeviceToDevice, s->stream));
+  PS_CUDA(cudaMemcpyAsync(p + 2 * vb, s->orig, ob, cudaMemcpyDeviceToDevice, s->stream));
+  return PS_OK;
+}
+
+extern "C" int ps_checkpoint_load(ps_sim* s, int32_t slot) {
+  if (s == nullptr) return fail(PS_ERR_INVALID, "ps_checkpoint_load: null simulation");
+  auto it = s->checkpoints.find(slot);
+  if (it == s->checkpoints.end()) return fail(PS_ERR_INVALID, "ps_checkpoint_load: empty slot " + std::to_string(slot));
+  DeviceGuard guard(s->device);
+  const size_t vb = (s->precision == PS_FP32 ? 16 : 32) * (size_t)s->n_total, ob = 4 * (size_t)s->n_total;
+  const char* p = static_cast<const char*>(it->second);
+  PS_CUDA(cudaMemcpyAsync(s->P0, p, vb, cudaMemcpyDeviceToDevice, s->stream));
+  PS_CUDA(cudaMemcpyAsync(s->V1, p + vb, vb, cudaMemcpyDeviceToDevice, s->stream));
+  PS_CUDA(cudaMemcpyAsync(s->orig, p + 2 * vb, ob, cudaMemcpyDeviceToDevice, s->stream));
+  s->grid_valid = false;
+  return PS_OK;
+}
+
+extern "C" int ps_time_steps(ps_sim* s, int64_t n_steps, double* device_ms) {
+  if (s == nullptr || device_ms == nullptr) return fail(PS_ERR_INVALID, "ps_time_steps: bad argument");
+  DeviceGuard guard(s->device);
+  cudaEvent_t a, b;
+  PS_CUDA(cudaEventCreate(&a));
+  PS_CUDA(cudaEventCreate(&b));
+  PS_CUDA(cudaEventRecord(a, s->stream));
+  int rc = ps_step(s, n_steps);
+  cudaEventRecord(b, s->stream);
+  cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc != PS_OK) return rc;
+  *device_ms = (double)ms;
+  return check_device_error(s);
+}
+
+extern "C" int ps_profile_steps(ps_sim* s, int64_t n_steps, double* kernel_ms, int64_t* kernel_launches) {
+  if (s == nullptr || kernel_ms == nullptr || kernel_launches == nullptr || n_steps < 1)
+    return fail(PS_ERR_INVALID, "ps_profile_steps: bad argument");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_profile_steps: call ps_set_state first");
+  for (int k = 0; k < PS_K_COUNT; ++k) {
+    kernel_ms[k] = 0.0;
+    kernel_launches[k] = 0;
+  }
+  if (s->n_total == 0) return PS_OK;
+  DeviceGuard guard(s->device);
+  std::vector<LaunchRecord> rec((size_t)(1 + 4 * n_steps));
+  for (auto& r : rec) {
+    PS_CUDA(cudaEventCreate(&r.a));
+    PS_CUDA(cudaEventCreate(&r.b));
+  }
+  if (s->precision == PS_FP32)
+    enqueue_steps_recorded_dispatch<float>(s, n_steps, rec);
+  else
+    enqueue_steps_recorded_dispatch<double>(s, n_steps, rec);
+  const cudaError_t le = cudaGetLastError();
+  cudaStreamSynchronize(s->stream);
+  for (auto& r : rec) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    kernel_ms[r.kind] += (double)ms;
+    kernel_launches[r.kind] += 1;
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  if (le != cudaSuccess) return fail(PS_ERR_CUDA, std::string("ps_profile_steps: ") + cudaGetErrorString(le));
+  s->grid_valid = true;
+  return check_device_error(s);
+}
+
+extern "C" int ps_sync(ps_sim* s) {
+  if (s == nullptr) return fail(PS_ERR_INVALID, "ps_sync: null simulation");
+  DeviceGuard guard(s->device);
+  PS_CUDA(cudaStreamSynchronize(s->stream));
+  return check_device_error(s);
+}
+
+extern "C" int64_t ps_last_launch_count(ps_sim* s) { return s ? s->last_launches : -1; }
+
+extern "C" int ps_grid_get(ps_sim* s, int32_t scene, ps_grid_info* out) {
+  if (s == nullptr || out == nullptr || scene < 0 || scene >= s->n_scenes) return fail(PS_ERR_INVALID, "ps_grid_get: bad argument");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_grid_get: no state uploaded");
+  const GridHost& g = s->grids[scene];
+  for (int a = 0; a < 3; ++a) {
+    out->min[a] = g.min[a];
+    out->nb[a] = g.nb[a];
+  }
+  out->interval = g.interval;
+  out->n_cells = g.n_cells;
+  out->cell_base = g.cbase;
+  out->particle_base = s->pbase[scene];
+  return PS_OK;
+}
+
+extern "C" int ps_buckets_get(ps_sim* s, uint32_t* counts, uint32_t* offsets, uint32_t* order) {
+  if (s == nullptr) return fail(PS_ERR_INVALID, "ps_buckets_get: null simulation");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_buckets_get: no state uploaded");
+  DeviceGuard guard(s->device);
+  if (!s->grid_valid) {
+    const int rc = regrid(s);
+    if (rc != PS_OK) return rc;
+  }
+  if (counts != nullptr && s->c_total > 0) {
+    // the count array itself is cleared during the step; derive it from the offsets
+    uint32_t* d = nullptr;
+    PS_CUDA(cudaMallocAsync(&d, sizeof(uint32_t) * s->c_total, s->stream));
+    k_counts_from_offsets<<<(unsigned)((s->c_total + 255) / 256), 256, 0, s->stream>>>(s->offset, d, s->c_total);
+    cudaMemcpyAsync(counts, d, sizeof(uint32_t) * s->c_total, cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(d, s->stream);
+    PS_CUDA(cudaGetLastError());
+  }
+  if (offsets != nullptr && s->c_total > 0)
+    PS_CUDA(cudaMemcpyAsync(offsets, s->offset, sizeof(uint32_t) * s->c_total, cudaMemcpyDeviceToHost, s->stream));
+  if (order != nullptr && s->n_total > 0)
+    PS_CUDA(cudaMemcpyAsync(order, s->orig, sizeof(uint32_t) * s->n_total, cudaMemcpyDeviceToHost, s->stream));
+  PS_CUDA(cudaStreamSynchronize(s->stream));
+  return check_device_error(s);
+}
+
+extern "C" int ps_stats_get(ps_sim* s, int32_t scene, ps_stats* out) {
+  if (s == nullptr || out == nullptr || scene < 0 || scene >= s->n_scenes) return fail(PS_ERR_INVALID, "ps_stats_get: bad argument");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_stats_get: no state uploaded");
+  DeviceGuard guard(s->device);
+  std::memset(out, 0, sizeof(*out));
+  const int64_t n = s->pbase[scene + 1] - s->pbase[scene];
+  if (n == 0) return PS_OK;
+  if (!s->grid_valid) {
+    const int rc = regrid(s);
+    if (rc != PS_OK) return rc;
+  }
+  const uint32_t first = (uint32_t)s->pbase[scene];
+  if (s->precision == PS_FP32) {
+    k_stats<float><<<kStatsBlocks, kStatsThreads, 0, s->stream>>>(bufs<float>(s), s->sp32[scene], first, (uint32_t)n, s->d_stats);
+  } else {
+    k_stats<double><<<kStatsBlocks, kStatsThreads, 0, s->stream>>>(bufs<double>(s), s->sp64[scene], first, (uint32_t)n, s->d_stats);
+  }
+  k_stats_final<<<1, 32, 0, s->stream>>>(s->d_stats, s->d_stats_out);
+  PS_CUDA(cudaGetLastError());
+  StatsPartial h{};
+  PS_CUDA(cudaMemcpyAsync(&h, s->d_stats_out, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  PS_CUDA(cudaStreamSynchronize(s->stream));
+  out->kinetic_energy = h.ke;
+  for (int a = 0; a < 3; ++a) {
+    out->min_pos[a] = h.mn[a];
+    out->max_pos[a] = h.mx[a];
+  }
+  out->n_collided = (int64_t)h.collided;
+  out->max_overlap = h.max_overlap;
+  return check_device_error(s);
+}
+
+extern "C" int ps_destroy(ps_sim* s) {
+  if (s == nullptr) return PS_OK;
+  {
+    DeviceGuard guard(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    free_sim(s);
+  }
+  delete s;
+  return PS_OK;
+}
+
+extern "C" int ps_simulate(const ps_scene_desc* scene, const double* aos_in, double* aos_out, int64_t max_steps,
+                           int32_t precision) {
+  if (scene == nullptr || max_steps < 0) return fail(PS_ERR_INVALID, "ps_simulate: bad argument");
+  ps_sim* s = nullptr;
+  int rc = ps_create(scene, 1, precision, 0, &s);
+  if (rc != PS_OK) return rc;
+  rc = ps_set_state(s, aos_in, scene->n_particles);
+  if (rc == PS_OK) rc = ps_step(s, max_steps);
+  if (rc == PS_OK) rc = ps_get_state(s, aos_out, scene->n_particles);
+  ps_destroy(s);
+  return rc;
+}
+
+extern "C" size_t ps_exclusive_scan_scratch_bytes(int64_t n) { return n <= 0 ? 8 : scan_scratch_bytes(n); }
+
+extern "C" int ps_exclusive_scan_u32(const uint32_t* d_in, uint32_t* d_out, int64_t n, void* d_scratch, void* stream) {
+  if (n < 0 || (n > 0 && (d_in == nullptr || d_out == nullptr || d_scratch == nullptr)))
+    return fail(PS_ERR_INVALID, "ps_exclusive_scan_u32: bad argument");
+  if (n == 0) return PS_OK;
+  if (n > (int64_t)1 << 40) return fail(PS_ERR_INVALID, "ps_exclusive_scan_u32: n too large");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // scratch: [uint32 ticket][uint32 error word][uint64 status per tile]
+  uint32_t* err = static_cast<uint32_t*>(d_scratch) + 1;
+  PS_CUDA(cudaMemsetAsync(d_scratch, 0, scan_scratch_bytes(n), st));
+  k_exclusive_scan_u32<<<(unsigned)scan_num_tiles(n), SCAN_THREADS, 0, st>>>(d_in, d_out, n, static_cast<uint64_t*>(d_scratch),
+                                                                             err);
+  PS_CUDA(cudaGetLastError());
+  return PS_OK;
+}

@@ -1,0 +1,260 @@
+"""psb200 — Python binding of libparticle_stabilizer_cuda.so (ctypes).
+
+The library is the product: C-ABI entry points declared in
+include/particle_stabilizer_b200.h, every one of which runs on the GPU.  This
+module only marshals numpy arrays into those calls.  There is no CPU
+fallback: if the library is missing, importing `lib()` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .scenes import Scene  # noqa: F401
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libparticle_stabilizer_cuda.so")
+CLI_PATH = os.path.join(PKG_ROOT, "bin", "particle_stabilizer_main")
+
+PS_OK = 0
+PS_FP32, PS_FP64 = 0, 1
+
+# every symbol include/particle_stabilizer_b200.h declares
+EXPORTED = (
+    "ps_last_error", "ps_create", "ps_set_state", "ps_get_state", "ps_step", "ps_sync", "ps_stats_get",
+    "ps_grid_get", "ps_buckets_get", "ps_last_launch_count", "ps_destroy", "ps_simulate",
+    "ps_exclusive_scan_scratch_bytes", "ps_exclusive_scan_u32", "ps_read_csv", "ps_write_csv", "ps_read_obj",
+    "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "runSimulateCUDA",
+)
+KERNEL_KINDS = ("begin", "scan", "scatter", "rank_move", "contacts")
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("n_particles", C.c_int64), ("box_min", C.c_double * 3), ("box_max", C.c_double * 3),
+                ("gravity", C.c_double * 3), ("e_wall", C.c_double * 6), ("k_spring", C.c_double),
+                ("e_sphere", C.c_double), ("dt", C.c_double), ("cell_size", C.c_double),
+                ("tri", C.POINTER(C.c_double)), ("n_tri", C.c_int64), ("edge_quirk", C.c_int32),
+                ("widen_domain", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("kinetic_energy", C.c_double), ("min_pos", C.c_double * 3), ("max_pos", C.c_double * 3),
+                ("n_collided", C.c_int64), ("max_overlap", C.c_double)]
+
+
+class GridInfo(C.Structure):
+    _fields_ = [("min", C.c_double * 3), ("interval", C.c_double), ("nb", C.c_int32 * 3), ("n_cells", C.c_int64),
+                ("cell_base", C.c_int64), ("particle_base", C.c_int64)]
+
+
+class PSError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PSError(f"{LIB_PATH} is missing: build it with `make -C particle-stabilizer_b200`")
+        L = C.CDLL(LIB_PATH)
+        L.ps_last_error.restype = C.c_char_p
+        L.ps_create.argtypes = [C.POINTER(SceneDesc), C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+        L.ps_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+        L.ps_get_state.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+        L.ps_step.argtypes = [C.c_void_p, C.c_int64]
+        L.ps_sync.argtypes = [C.c_void_p]
+        L.ps_stats_get.argtypes = [C.c_void_p, C.c_int32, C.POINTER(Stats)]
+        L.ps_grid_get.argtypes = [C.c_void_p, C.c_int32, C.POINTER(GridInfo)]
+        L.ps_buckets_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ps_last_launch_count.argtypes = [C.c_void_p]
+        L.ps_last_launch_count.restype = C.c_int64
+        L.ps_destroy.argtypes = [C.c_void_p]
+        L.ps_simulate.argtypes = [C.POINTER(SceneDesc), C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]
+        L.ps_exclusive_scan_scratch_bytes.argtypes = [C.c_int64]
+        L.ps_exclusive_scan_scratch_bytes.restype = C.c_size_t
+        L.ps_exclusive_scan_u32.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+        L.ps_read_csv.argtypes = [C.c_char_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+        L.ps_write_csv.argtypes = [C.c_char_p, C.c_void_p, C.c_int64]
+        L.ps_read_obj.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+        L.ps_checkpoint_save.argtypes = [C.c_void_p, C.c_int32]
+        L.ps_checkpoint_load.argtypes = [C.c_void_p, C.c_int32]
+        L.ps_time_steps.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_double)]
+        L.ps_profile_steps.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != PS_OK:
+        raise PSError(f"{what} failed ({rc}): {lib().ps_last_error().decode()}")
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def precision_code(precision: str) -> int:
+    return {"f32": PS_FP32, "fp32": PS_FP32, "f64": PS_FP64, "fp64": PS_FP64}[precision]
+
+
+def scene_desc(sc: Scene, keep: list) -> SceneDesc:
+    d = SceneDesc()
+    d.n_particles = sc.n
+    d.box_min = (C.c_double * 3)(*sc.box_min)
+    d.box_max = (C.c_double * 3)(*sc.box_max)
+    d.gravity = (C.c_double * 3)(*sc.gravity)
+    d.e_wall = (C.c_double * 6)(*sc.e_wall)
+    d.k_spring = sc.k_spring
+    d.e_sphere = sc.e_sphere
+    d.dt = sc.dt
+    d.cell_size = sc.interval
+    if sc.tri is not None:
+        t = np.ascontiguousarray(sc.tri, dtype=np.float64)
+        keep.append(t)
+        d.tri = t.ctypes.data_as(C.POINTER(C.c_double))
+        d.n_tri = t.shape[0]
+    d.edge_quirk = sc.edge_quirk
+    d.widen_domain = sc.widen_domain
+    return d
+
+
+class Simulation:
+    """One or many scenes on one GPU (ps_create ... ps_destroy)."""
+
+    def __init__(self, scenes, precision: str = "f32", device: int = 0):
+        if isinstance(scenes, Scene):
+            scenes = [scenes]
+        self.scenes = list(scenes)
+        keep: list = []
+        arr = (SceneDesc * len(self.scenes))(*[scene_desc(s, keep) for s in self.scenes])
+        h = C.c_void_p()
+        _check(lib().ps_create(arr, len(self.scenes), precision_code(precision), device, C.byref(h)), "ps_create")
+        self.h = h
+        self.n = sum(s.n for s in self.scenes)
+        self.precision = precision
+
+    def set_state(self, state: np.ndarray | None = None) -> None:
+        if state is None:
+            state = np.concatenate([s.state for s in self.scenes]) if self.n else np.zeros((0, 8))
+        st = np.ascontiguousarray(state, dtype=np.float64)
+        _check(lib().ps_set_state(self.h, _ptr(st), st.shape[0]), "ps_set_state")
+
+    def get_state(self) -> np.ndarray:
+        out = np.empty((self.n, 8), dtype=np.float64)
+        _check(lib().ps_get_state(self.h, _ptr(out), self.n), "ps_get_state")
+        return out
+
+    def step(self, n_steps: int) -> None:
+        _check(lib().ps_step(self.h, int(n_steps)), "ps_step")
+
+    def sync(self) -> None:
+        _check(lib().ps_sync(self.h), "ps_sync")
+
+    def launches(self) -> int:
+        return int(lib().ps_last_launch_count(self.h))
+
+    def checkpoint_save(self, slot: int = 0) -> None:
+        _check(lib().ps_checkpoint_save(self.h, slot), "ps_checkpoint_save")
+
+    def checkpoint_load(self, slot: int = 0) -> None:
+        _check(lib().ps_checkpoint_load(self.h, slot), "ps_checkpoint_load")
+
+    def time_steps(self, n_steps: int) -> float:
+        """Device milliseconds of ps_step(n_steps), CUDA events on the simulation's stream."""
+        ms = C.c_double()
+        _check(lib().ps_time_steps(self.h, int(n_steps), C.byref(ms)), "ps_time_steps")
+        return float(ms.value)
+
+    def profile_steps(self, n_steps: int) -> dict:
+        """Per kernel kind: (summed device ms, launches) over n_steps eager steps."""
+        ms = np.zeros(len(KERNEL_KINDS), dtype=np.float64)
+        cnt = np.zeros(len(KERNEL_KINDS), dtype=np.int64)
+        _check(lib().ps_profile_steps(self.h, int(n_steps), _ptr(ms), _ptr(cnt)), "ps_profile_steps")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(KERNEL_KINDS)}
+
+    def stats(self, scene: int = 0) -> Stats:
+        s = Stats()
+        _check(lib().ps_stats_get(self.h, scene, C.byref(s)), "ps_stats_get")
+        return s
+
+    def grid(self, scene: int = 0) -> GridInfo:
+        g = GridInfo()
+        _check(lib().ps_grid_get(self.h, scene, C.byref(g)), "ps_grid_get")
+        return g
+
+    def buckets(self):
+        """(counts, offsets, order) over all cells / particles of all scenes."""
+        total = 0
+        for k in range(len(self.scenes)):
+            g = self.grid(k)
+            total = max(total, g.cell_base + g.n_cells)
+        counts = np.empty(total, dtype=np.uint32)
+        offsets = np.empty(total, dtype=np.uint32)
+        order = np.empty(self.n, dtype=np.uint32)
+        _check(lib().ps_buckets_get(self.h, _ptr(counts), _ptr(offsets), _ptr(order)), "ps_buckets_get")
+        return counts, offsets, order
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().ps_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def simulate(scene: Scene, steps: int, precision: str = "f32") -> np.ndarray:
+    """ps_simulate: runSimulateCUDA with host buffers."""
+    keep: list = []
+    d = scene_desc(scene, keep)
+    st = np.ascontiguousarray(scene.state, dtype=np.float64)
+    out = np.empty_like(st)
+    _check(lib().ps_simulate(C.byref(d), _ptr(st), _ptr(out), int(steps), precision_code(precision)), "ps_simulate")
+    return out
+
+
+def exclusive_scan_u32(d_in: int, d_out: int, n: int, d_scratch: int, stream: int = 0) -> None:
+    """ps_exclusive_scan_u32 on device pointers (integers)."""
+    _check(lib().ps_exclusive_scan_u32(C.c_void_p(d_in), C.c_void_p(d_out), int(n), C.c_void_p(d_scratch),
+                                       C.c_void_p(stream)), "ps_exclusive_scan_u32")
+
+
+def exclusive_scan_scratch_bytes(n: int) -> int:
+    return int(lib().ps_exclusive_scan_scratch_bytes(int(n)))
+
+
+def read_csv(path: str, velocity=(0.0, 0.0, -10.0), density: float = 1.0) -> np.ndarray:
+    n = C.c_int64()
+    v = (C.c_double * 3)(*velocity)
+    _check(lib().ps_read_csv(path.encode(), v, density, None, 0, C.byref(n)), "ps_read_csv")
+    out = np.empty((n.value, 8), dtype=np.float64)
+    _check(lib().ps_read_csv(path.encode(), v, density, _ptr(out), n.value, C.byref(n)), "ps_read_csv")
+    return out
+
+
+def write_csv(path: str, state: np.ndarray) -> None:
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    _check(lib().ps_write_csv(path.encode(), _ptr(st), st.shape[0]), "ps_write_csv")
+
+
+def read_obj(path: str) -> np.ndarray:
+    n = C.c_int64()
+    _check(lib().ps_read_obj(path.encode(), None, 0, C.byref(n)), "ps_read_obj")
+    out = np.empty((n.value, 9), dtype=np.float64)
+    _check(lib().ps_read_obj(path.encode(), _ptr(out), n.value, C.byref(n)), "ps_read_obj")
+    return out
