@@ -128,24 +128,24 @@ def barrier(dist):
         dist.barrier()
 
 
-def max_over_ranks(dist, x: float) -> float:
+def _reduce(dist, x: float, op) -> float:
     if dist is None:
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(dist, x: float) -> float:
+    """Largest value over the ranks (device time: the slowest rank sets it)."""
+    return _reduce(dist, x, dist.ReduceOp.MAX) if dist is not None else x
 
 
 def sum_over_ranks(dist, x: float) -> float:
-    if dist is None:
-        return x
-    import torch
-
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(dist, x, dist.ReduceOp.SUM) if dist is not None else x
 
 
 # algorithmic bytes per particle of each kernel (FP32 state = 2 x 16 B)

@@ -93,8 +93,34 @@ struct SceneParams {
   T mesh_lo[3];            // triangle-bin grid origin
   T mesh_iv;               // triangle-bin edge
   int32_t edge_quirk;
-  int32_t pad_;
+  // unsigned division by nz and by ny with a multiply-high (Granlund &
+  // Montgomery): q = (t + ((x - t) >> sh1)) >> sh2, t = umulhi(x, m)
+  uint32_t div_nz_m, div_nz_sh1, div_nz_sh2;
+  uint32_t div_ny_m, div_ny_sh1, div_ny_sh2;
+  // cell boundaries: axis a of this scene uses bounds[bnd_base[a] + k] for
+  // k = 0..nb[a]; the clamped cell index of x is k exactly when
+  // bounds[k] <= x < bounds[k+1] (bounds[0] = -inf, bounds[nb] = +inf)
+  uint32_t bnd_base[3];
 };
+
+__host__ __device__ inline uint32_t fast_udiv(uint32_t x, uint32_t m, uint32_t sh1, uint32_t sh2) {
+#ifdef __CUDA_ARCH__
+  const uint32_t t = __umulhi(x, m);
+#else
+  const uint32_t t = (uint32_t)(((uint64_t)x * m) >> 32);
+#endif
+  return (t + ((x - t) >> sh1)) >> sh2;
+}
+
+// Magic numbers of fast_udiv for a divisor d >= 1: l = ceil(log2 d),
+// m = floor(2^32 (2^l - d) / d) + 1, sh1 = min(l, 1), sh2 = max(l - 1, 0).
+inline void fast_udiv_magic(uint32_t d, uint32_t& m, uint32_t& sh1, uint32_t& sh2) {
+  uint32_t l = 0;
+  while (l < 32 && (1ull << l) < d) ++l;
+  m = (uint32_t)((((uint64_t)1 << 32) * (((uint64_t)1 << l) - d)) / d + 1);
+  sh1 = l < 1 ? l : 1;
+  sh2 = l > 1 ? l - 1 : 0;
+}
 
 // Device error word bits (read by the host after a step block).
 enum : uint32_t {

@@ -11,7 +11,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <string>
 #include <vector>
@@ -91,9 +93,10 @@ struct ps_sim {
   void* part_arena = nullptr;
   void* cell_arena = nullptr;
   void *P0 = nullptr, *V0 = nullptr, *P1 = nullptr, *V1 = nullptr;
-  uint32_t *orig = nullptr, *cell = nullptr, *slot = nullptr, *tmp = nullptr;
+  uint32_t *orig = nullptr, *cell = nullptr, *slot = nullptr, *tmp = nullptr, *scell = nullptr;
   uint32_t *count = nullptr, *offset = nullptr, *err = nullptr, *d_pbase = nullptr;
-  uint64_t* scan_scratch = nullptr;
+  uint32_t* tile_sum = nullptr;  // per-tile totals of `count` for the step's scan
+  void* d_bounds = nullptr;       // per-scene, per-axis cell boundaries in the state precision
   double* staging = nullptr;  // n_total x 8 doubles
   void* d_scenes = nullptr;
   StatsPartial* d_stats = nullptr;
@@ -109,6 +112,8 @@ struct ps_sim {
   std::map<int64_t, cudaGraphExec_t> graphs;
   int64_t last_launches = 0;
   std::map<int32_t, void*> checkpoints;  // slot -> device copy of (P0, V1, orig)
+  cudaAccessPolicyWindow l2_window{};     // count + offset arrays kept in L2
+  bool l2_window_on = false;
 };
 
 namespace {
@@ -116,7 +121,6 @@ namespace {
 constexpr int64_t kGraphBlock = 200;  // steps per captured graph
 
 int64_t n_scan(const ps_sim* s) { return s->c_total + 1; }
-uint32_t scan_words(const ps_sim* s) { return (uint32_t)(scan_num_tiles(n_scan(s)) + 1); }
 
 template <class T>
 StepBufs<T> bufs(ps_sim* s) {
@@ -136,8 +140,10 @@ StepBufs<T> bufs(ps_sim* s) {
   b.pbase = s->d_pbase;
   b.n_scenes = s->n_scenes;
   b.n = (uint32_t)s->n_total;
-  b.scan_scratch = s->scan_scratch;
-  b.scan_words = scan_words(s);
+  b.tile_sum = s->tile_sum;
+  b.scell = s->scell;
+  b.bounds = static_cast<const T*>(s->d_bounds);
+  b.n_tiles = (uint32_t)scan_num_tiles(n_scan(s));
   return b;
 }
 
@@ -153,13 +159,19 @@ const std::vector<SceneParams<double>>& params<double>(const ps_sim* s) {
 }
 
 unsigned blocks_for(int64_t n) { return (unsigned)((n + STEP_THREADS - 1) / STEP_THREADS); }
+// grid of k_scatter / k_rank_move: MOVE_PER_THREAD particles per thread, and
+// at least one thread per scan-scratch word
+unsigned move_blocks(int64_t n, uint32_t words) {
+  const int64_t per = (int64_t)STEP_THREADS * MOVE_PER_THREAD;
+  return (unsigned)std::max<int64_t>((n + per - 1) / per, (words + STEP_THREADS - 1) / STEP_THREADS);
+}
 
 // ---- the launch sequence -----------------------------------------------------
 template <class T, bool MULTI, bool MESH>
 int64_t enqueue_steps(ps_sim* s, int64_t steps) {
   const StepBufs<T> b = bufs<T>(s);
   const SceneParams<T> sp0 = params<T>(s)[0];
-  const unsigned gb = blocks_for(std::max<int64_t>(s->n_total, scan_words(s)));
+  const unsigned gb = blocks_for(s->n_total);
   const unsigned gp = blocks_for(s->n_total);
   const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
   cudaStream_t st = s->stream;
@@ -167,10 +179,10 @@ int64_t enqueue_steps(ps_sim* s, int64_t steps) {
   k_begin<T, MULTI, MESH, true><<<gb, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
   ++launches;
   for (int64_t k = 0; k < steps; ++k) {
-    k_exclusive_scan_u32<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->scan_scratch, s->err);
-    k_scatter<<<gb, STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp, s->count,
-                                           (uint32_t)s->n_total, s->scan_scratch, scan_words(s));
-    k_rank_move<T><<<gp, STEP_THREADS, 0, st>>>(b);
+    k_scan_with_tile_sums<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->tile_sum);
+    k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
+                                                                         s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
+    k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
     if (k + 1 < steps)
       k_contacts<T, MULTI, MESH, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
     else
@@ -190,7 +202,7 @@ template <class T, bool MULTI, bool MESH>
 void enqueue_steps_recorded(ps_sim* s, int64_t steps, std::vector<LaunchRecord>& rec) {
   const StepBufs<T> b = bufs<T>(s);
   const SceneParams<T> sp0 = params<T>(s)[0];
-  const unsigned gb = blocks_for(std::max<int64_t>(s->n_total, scan_words(s)));
+  const unsigned gb = blocks_for(s->n_total);
   const unsigned gp = blocks_for(s->n_total);
   const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
   cudaStream_t st = s->stream;
@@ -205,14 +217,14 @@ void enqueue_steps_recorded(ps_sim* s, int64_t steps, std::vector<LaunchRecord>&
   post();
   for (int64_t k = 0; k < steps; ++k) {
     pre(PS_K_SCAN);
-    k_exclusive_scan_u32<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->scan_scratch, s->err);
+    k_scan_with_tile_sums<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->tile_sum);
     post();
     pre(PS_K_SCATTER);
-    k_scatter<<<gb, STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp, s->count,
-                                           (uint32_t)s->n_total, s->scan_scratch, scan_words(s));
+    k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
+                                                                         s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
     post();
     pre(PS_K_RANK_MOVE);
-    k_rank_move<T><<<gp, STEP_THREADS, 0, st>>>(b);
+    k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
     post();
     pre(PS_K_CONTACTS);
     if (k + 1 < steps)
@@ -252,15 +264,15 @@ template <class T, bool MULTI>
 void enqueue_regrid(ps_sim* s) {
   const StepBufs<T> b = bufs<T>(s);
   const SceneParams<T> sp0 = params<T>(s)[0];
-  const unsigned gb = blocks_for(std::max<int64_t>(s->n_total, scan_words(s)));
+  const unsigned gb = blocks_for(s->n_total);
   const unsigned gp = blocks_for(s->n_total);
   cudaStream_t st = s->stream;
   k_begin<T, MULTI, false, false><<<gb, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
-  k_exclusive_scan_u32<<<(unsigned)scan_num_tiles(n_scan(s)), SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s),
-                                                                                    s->scan_scratch, s->err);
-  k_scatter<<<gb, STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp, s->count,
-                                         (uint32_t)s->n_total, s->scan_scratch, scan_words(s));
-  k_rank_move<T><<<gp, STEP_THREADS, 0, st>>>(b);
+  k_scan_with_tile_sums<<<(unsigned)scan_num_tiles(n_scan(s)), SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s),
+                                                                                     s->tile_sum);
+  k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
+                                                                       s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
+  k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
   k_copy_vel<T><<<gp, STEP_THREADS, 0, st>>>(b);
 }
 
@@ -369,6 +381,8 @@ SceneParams<T> make_params(const ps_scene_desc& d, const GridHost& g, int64_t pb
   sp.mesh_bin_base = (uint32_t)g.bin_base;
   sp.mesh_iv = (T)g.mesh_iv;
   sp.edge_quirk = d.edge_quirk;
+  fast_udiv_magic((uint32_t)std::max(1, g.nb[2]), sp.div_nz_m, sp.div_nz_sh1, sp.div_nz_sh2);
+  fast_udiv_magic((uint32_t)std::max(1, g.nb[1]), sp.div_ny_m, sp.div_ny_sh1, sp.div_ny_sh2);
   return sp;
 }
 
@@ -379,6 +393,85 @@ int32_t host_mesh_axis(T x, T lo, T iv, int32_t nb) {
   if (!(q > T(0))) return 0;
   if (q >= (T)nb) return nb - 1;
   return (int32_t)q;
+}
+
+// Host copy of the device's axis_cell (same IEEE operations in T).
+template <class T>
+int32_t host_axis_cell(T x, T lo, T iv, int32_t nb) {
+  const T q = (x - lo) / iv;
+  if (!(q > T(0))) return 0;
+  if (q >= (T)nb) return nb - 1;
+  return (int32_t)q;
+}
+
+// Order-preserving map between finite/infinite T and unsigned integers.
+inline uint64_t key_of(double x) {
+  uint64_t u;
+  std::memcpy(&u, &x, 8);
+  return (u >> 63) ? ~u : (u | (1ull << 63));
+}
+inline double val_of(double, uint64_t k) {
+  const uint64_t u = (k >> 63) ? (k & ~(1ull << 63)) : ~k;
+  double x;
+  std::memcpy(&x, &u, 8);
+  return x;
+}
+inline uint32_t key_of(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  return (u >> 31) ? ~u : (u | (1u << 31));
+}
+inline float val_of(float, uint32_t k) {
+  const uint32_t u = (k >> 31) ? (k & ~(1u << 31)) : ~k;
+  float x;
+  std::memcpy(&x, &u, 4);
+  return x;
+}
+
+// Boundaries B[0..nb] of one axis: B[k] is the smallest T with
+// host_axis_cell(x) >= k (bisection over the ordered bit patterns, since the
+// cell index is monotonic in x); B[0] = -inf, B[nb] = +inf.  Checked.
+template <class T>
+bool axis_bounds(T lo, T iv, int32_t nb, std::vector<T>& out) {
+  using K = decltype(key_of(T(0)));
+  const T inf = std::numeric_limits<T>::infinity();
+  out.push_back(-inf);
+  for (int32_t k = 1; k < nb; ++k) {
+    K a = key_of(-inf), b = key_of(inf);  // f(val(a)) < k <= f(val(b))
+    while (b - a > 1) {
+      const K m = a + (b - a) / 2;
+      if (host_axis_cell<T>(val_of(T(0), m), lo, iv, nb) >= k)
+        b = m;
+      else
+        a = m;
+    }
+    const T x = val_of(T(0), b);
+    if (host_axis_cell<T>(x, lo, iv, nb) != k || host_axis_cell<T>(val_of(T(0), b - 1), lo, iv, nb) != k - 1)
+      return false;
+    out.push_back(x);
+  }
+  out.push_back(inf);
+  return true;
+}
+
+template <class T>
+int upload_bounds(ps_sim* s) {
+  std::vector<T> all;
+  for (int sc = 0; sc < s->n_scenes; ++sc) {
+    const GridHost& g = s->grids[sc];
+    for (int a = 0; a < 3; ++a) {
+      const uint32_t base = (uint32_t)all.size();
+      if (!axis_bounds<T>((T)g.min[a], (T)g.interval, g.nb[a], all))
+        return fail(PS_ERR_INVALID, "cell boundary table is not monotonic on axis " + std::to_string(a));
+      if (s->precision == PS_FP32)
+        s->sp32[sc].bnd_base[a] = base;
+      else
+        s->sp64[sc].bnd_base[a] = base;
+    }
+  }
+  PS_CUDA(cudaMalloc(&s->d_bounds, sizeof(T) * all.size()));
+  PS_CUDA(cudaMemcpy(s->d_bounds, all.data(), sizeof(T) * all.size(), cudaMemcpyHostToDevice));
+  return PS_OK;
 }
 
 // Triangle data in precision T for every scene, binned by AABB.
@@ -453,6 +546,54 @@ int upload_mesh(ps_sim* s) {
   const MeshView mv{s->d_tri, s->d_nrm, s->d_aabb, s->d_bin_offset, s->d_bin_tri};
   PS_CUDA(cudaMemcpy(s->d_mesh_view, &mv, sizeof(MeshView), cudaMemcpyHostToDevice));
   return PS_OK;
+}
+
+// Keep the per-cell count and offset arrays resident in L2: they take
+// scattered atomics, scattered clears and random offset reads every step,
+// while the particle arrays stream through.  The persisting carve-out is a
+// limit of this process's CUDA context only.
+void setup_l2_window(ps_sim* s, size_t bytes) {
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, s->device) != cudaSuccess) return;
+  if (prop.persistingL2CacheMaxSize <= 0 || prop.accessPolicyMaxWindowSize <= 0) return;
+  if (std::getenv("PSB200_NO_L2_WINDOW") != nullptr) return;
+  const size_t win = std::min<size_t>(bytes, (size_t)prop.accessPolicyMaxWindowSize);
+  size_t cur = 0;
+  cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+  const size_t want = std::min<size_t>((size_t)prop.persistingL2CacheMaxSize, win);
+  if (cur < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+  s->l2_window.base_ptr = s->cell_arena;
+  s->l2_window.num_bytes = win;
+  s->l2_window.hitRatio = (float)std::min(1.0, (double)cur / (double)win);
+  s->l2_window.hitProp = cudaAccessPropertyPersisting;
+  s->l2_window.missProp = cudaAccessPropertyStreaming;
+  cudaStreamAttrValue v{};
+  v.accessPolicyWindow = s->l2_window;
+  if (cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &v) == cudaSuccess)
+    s->l2_window_on = true;
+  else
+    cudaGetLastError();
+}
+
+// Captured kernel nodes carry the window explicitly.
+void apply_l2_window(ps_sim* s, cudaGraph_t g) {
+  if (!s->l2_window_on) return;
+  size_t n = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return;
+  std::vector<cudaGraphNode_t> nodes(n);
+  cudaGraphGetNodes(g, nodes.data(), &n);
+  cudaKernelNodeAttrValue v{};
+  v.accessPolicyWindow = s->l2_window;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+      cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributeAccessPolicyWindow, &v);
+  }
+  cudaGetLastError();
 }
 
 // Size every scene's grid from its radii and allocate the per-cell arrays.
@@ -547,15 +688,14 @@ int size_grids(ps_sim* s, const double* aos) {
 
   // per-cell arrays and scan scratch
   const size_t cells_b = align_up(sizeof(uint32_t) * (size_t)(s->c_total + 1), 256);
-  const size_t scratch_b = align_up(scan_scratch_bytes(n_scan(s)), 256);
-  PS_CUDA(cudaMalloc(&s->cell_arena, 2 * cells_b + scratch_b));
+  const size_t tiles_b = align_up(sizeof(uint32_t) * (size_t)scan_num_tiles(n_scan(s)), 256);
+  PS_CUDA(cudaMalloc(&s->cell_arena, 2 * cells_b + tiles_b));
   char* c = static_cast<char*>(s->cell_arena);
   s->count = reinterpret_cast<uint32_t*>(c);
   s->offset = reinterpret_cast<uint32_t*>(c + cells_b);
-  s->scan_scratch = reinterpret_cast<uint64_t*>(c + 2 * cells_b);
-  PS_CUDA(cudaMemset(s->count, 0, cells_b));
-  PS_CUDA(cudaMemset(s->offset, 0, cells_b));
-  PS_CUDA(cudaMemset(s->scan_scratch, 0, scratch_b));
+  s->tile_sum = reinterpret_cast<uint32_t*>(c + 2 * cells_b);
+  PS_CUDA(cudaMemset(s->cell_arena, 0, 2 * cells_b + tiles_b));
+  setup_l2_window(s, 2 * cells_b + tiles_b);
 
   // scene parameter tables
   s->sp32.clear();
@@ -564,6 +704,10 @@ int size_grids(ps_sim* s, const double* aos) {
     const int64_t pc = s->pbase[sc + 1] - s->pbase[sc];
     s->sp32.push_back(make_params<float>(s->desc[sc], s->grids[sc], s->pbase[sc], pc));
     s->sp64.push_back(make_params<double>(s->desc[sc], s->grids[sc], s->pbase[sc], pc));
+  }
+  {
+    const int rc = s->precision == PS_FP32 ? upload_bounds<float>(s) : upload_bounds<double>(s);
+    if (rc != PS_OK) return rc;
   }
   const size_t spb = s->precision == PS_FP32 ? sizeof(SceneParams<float>) : sizeof(SceneParams<double>);
   PS_CUDA(cudaMalloc(&s->d_scenes, spb * s->n_scenes));
@@ -580,6 +724,13 @@ int size_grids(ps_sim* s, const double* aos) {
 }
 
 void free_sim(ps_sim* s) {
+  if (s->l2_window_on) {
+    cudaStreamAttrValue v{};
+    v.accessPolicyWindow.num_bytes = 0;
+    cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &v);
+    cudaCtxResetPersistingL2Cache();
+    cudaGetLastError();
+  }
   for (auto& kv : s->checkpoints) cudaFree(kv.second);
   s->checkpoints.clear();
   for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
@@ -587,6 +738,7 @@ void free_sim(ps_sim* s) {
   cudaFree(s->part_arena);
   cudaFree(s->cell_arena);
   cudaFree(s->d_scenes);
+  cudaFree(s->d_bounds);
   cudaFree(s->d_tri);
   cudaFree(s->d_nrm);
   cudaFree(s->d_aabb);
@@ -641,7 +793,7 @@ extern "C" int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t 
   const size_t n = (size_t)std::max<int64_t>(s->n_total, 1);
   const size_t b4 = align_up(vb * n, 256), bu = align_up(4 * n, 256), bs = align_up(64 * n, 256);
   const size_t bp = align_up(4 * (size_t)(n_scenes + 1), 256);
-  cudaError_t e = cudaMalloc(&s->part_arena, 4 * b4 + 4 * bu + bs + 256 + bp + 2 * sizeof(StatsPartial) * kStatsBlocks + 256);
+  cudaError_t e = cudaMalloc(&s->part_arena, 4 * b4 + 5 * bu + bs + 256 + bp + 2 * sizeof(StatsPartial) * kStatsBlocks + 256);
   if (e != cudaSuccess) {
     delete s;
     return fail(e == cudaErrorMemoryAllocation ? PS_ERR_NOMEM : PS_ERR_CUDA, std::string("ps_create: ") + cudaGetErrorString(e));
@@ -655,6 +807,7 @@ extern "C" int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t 
   s->cell = reinterpret_cast<uint32_t*>(p); p += bu;
   s->slot = reinterpret_cast<uint32_t*>(p); p += bu;
   s->tmp = reinterpret_cast<uint32_t*>(p); p += bu;
+  s->scell = reinterpret_cast<uint32_t*>(p); p += bu;
   s->staging = reinterpret_cast<double*>(p); p += bs;
   s->err = reinterpret_cast<uint32_t*>(p); p += 256;
   s->d_pbase = reinterpret_cast<uint32_t*>(p); p += bp;
@@ -743,6 +896,7 @@ extern "C" int ps_step(ps_sim* s, int64_t n_steps) {
         if (graph) cudaGraphDestroy(graph);
         return fail(PS_ERR_CUDA, std::string("ps_step: capture failed: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee));
       }
+      apply_l2_window(s, graph);
       cudaGraphExec_t exec = nullptr;
       const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
       cudaGraphDestroy(graph);

@@ -3,15 +3,15 @@
 // scan (src/ParticleStabilizerCUDA/PrefixScan.cu:113-268), which allocates
 // and frees block-sum arrays every step once the grid passes 2^20 cells.
 //
-// One launch, one read and one write per element: each CTA takes a tile of
+// One launch, one read and one write per element.  Each CTA takes a tile of
 // SCAN_TILE elements in ticket order (an atomic counter, so every
-// predecessor tile is already running), publishes its aggregate, then warp 0
-// walks back over the predecessors' status words 32 at a time until it meets
-// an inclusive prefix.  A status word packs (value << 32 | flag) so value and
-// flag travel in one 64-bit store.  The wait on a predecessor is bounded:
-// after SCAN_SPIN_LIMIT polls the tile records PS_DEVERR_SCAN_TIMEOUT in the
-// error word, takes the missing value as 0 and finishes, so the kernel always
-// returns.
+// predecessor tile is already running), publishes its aggregate, then all
+// its threads look back over 256 predecessor status words per round until
+// one holds an inclusive prefix.  A status word packs (value << 32 | flag)
+// so value and flag travel in one 64-bit store.  Every wait on a predecessor
+// is bounded: after SCAN_SPIN_LIMIT polls the thread records
+// PS_DEVERR_SCAN_TIMEOUT in the error word and takes the missing value as 0,
+// so the kernel always returns.
 #pragma once
 
 #include <cuda/atomic>
@@ -21,7 +21,7 @@
 namespace psb {
 
 constexpr int SCAN_THREADS = 256;
-constexpr int SCAN_ITEMS = 16;  // per thread: 64 contiguous bytes
+constexpr int SCAN_ITEMS = 32;  // per thread: 128 contiguous bytes
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr uint32_t SCAN_SPIN_LIMIT = 1u << 20;
 
@@ -39,11 +39,10 @@ __device__ __forceinline__ void scan_st(uint64_t* p, uint64_t v) {
 }
 
 // in and out may alias.  `scratch` must be zeroed before the launch.
-__global__ void __launch_bounds__(SCAN_THREADS) k_exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n,
+__global__ void __launch_bounds__(SCAN_THREADS, 8) k_exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n,
                                                                      uint64_t* scratch, uint32_t* err) {
   __shared__ uint32_t s_warp[SCAN_THREADS / 32];
   __shared__ uint32_t s_tile;
-  __shared__ uint32_t s_prefix;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   uint64_t* status = scratch + 1;
 
@@ -52,24 +51,20 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_exclusive_scan_u32(const uint3
   const int64_t tile = s_tile;
   const int64_t base = tile * SCAN_TILE + (int64_t)tid * SCAN_ITEMS;
 
-  uint32_t v[SCAN_ITEMS];
-  if (base + SCAN_ITEMS <= n && (((uintptr_t)(in + base)) & 15) == 0) {
+  // pass 1: per-thread sum only (values are re-read after the look-back, from
+  // L1/L2, so a CTA holds few registers and every tile is resident at once)
+  const bool vec = base + SCAN_ITEMS <= n && (((uintptr_t)(in + base)) & 15) == 0;
+  uint32_t local = 0;
+  if (vec) {
     const uint4* q = reinterpret_cast<const uint4*>(in + base);
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS / 4; ++k) {
       const uint4 w = q[k];
-      v[4 * k + 0] = w.x;
-      v[4 * k + 1] = w.y;
-      v[4 * k + 2] = w.z;
-      v[4 * k + 3] = w.w;
+      local += w.x + w.y + w.z + w.w;
     }
   } else {
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k) v[k] = (base + k < n) ? in[base + k] : 0u;
+    for (int k = 0; k < SCAN_ITEMS; ++k) local += (base + k < n) ? in[base + k] : 0u;
   }
-  uint32_t local = 0;
-#pragma unroll
-  for (int k = 0; k < SCAN_ITEMS; ++k) local += v[k];
 
   // warp-inclusive scan of the per-thread sums
   uint32_t inc = local;
@@ -88,60 +83,164 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_exclusive_scan_u32(const uint3
     tile_sum += t;
   }
 
-  // publish and look back
+  // publish the aggregate, then warp 0 looks back 32 predecessors per round
+  __shared__ uint32_t s_prefix;
   if (warp == 0) {
     uint32_t prefix = 0;
     if (tile == 0) {
       if (lane == 0) scan_st(&status[0], ((uint64_t)tile_sum << 32) | SCAN_FLAG_PREFIX);
     } else {
       if (lane == 0) scan_st(&status[tile], ((uint64_t)tile_sum << 32) | SCAN_FLAG_AGG);
-      int64_t pred = tile - 1;  // nearest predecessor handled by lane 0
-      bool done = false;
+      int64_t pred = tile - 1;  // predecessor read by lane 0 this round
       uint32_t spins = 0;
-      while (!done) {
+      bool timed_out = false;
+      while (true) {
         const int64_t idx = pred - lane;
         uint64_t s = (idx >= 0) ? scan_ld(&status[idx]) : (uint64_t)SCAN_FLAG_PREFIX;
+        unsigned ns = 32;
         while (__any_sync(0xffffffffu, (s & 3u) == SCAN_FLAG_NONE)) {
           if (++spins > SCAN_SPIN_LIMIT) {
-            if (lane == 0) atomicOr(err, PS_DEVERR_SCAN_TIMEOUT);
+            timed_out = true;
             if ((s & 3u) == SCAN_FLAG_NONE) s = (uint64_t)SCAN_FLAG_PREFIX;  // give up: value 0
             break;
           }
+          __nanosleep(ns);
+          ns = ns < 512 ? 2 * ns : 512;
           if ((s & 3u) == SCAN_FLAG_NONE) s = scan_ld(&status[idx]);
         }
-        const uint32_t flag = (uint32_t)(s & 3u);
-        const uint32_t val = (uint32_t)(s >> 32);
-        const unsigned pmask = __ballot_sync(0xffffffffu, flag == SCAN_FLAG_PREFIX);
-        // lanes up to and including the first inclusive prefix contribute
-        const int stop = pmask ? (__ffs(pmask) - 1) : 31;
-        uint32_t contrib = (lane <= stop) ? val : 0u;
+        const unsigned pm = __ballot_sync(0xffffffffu, (s & 3u) == SCAN_FLAG_PREFIX);
+        const int stop = pm ? (__ffs(pm) - 1) : 31;
+        uint32_t contrib = (lane <= stop) ? (uint32_t)(s >> 32) : 0u;
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, d);
         prefix += contrib;
-        done = (pmask != 0);
+        if (pm) break;
         pred -= 32;
       }
+      if (timed_out && lane == 0) atomicOr(err, PS_DEVERR_SCAN_TIMEOUT);
       if (lane == 0) scan_st(&status[tile], ((uint64_t)(prefix + tile_sum) << 32) | SCAN_FLAG_PREFIX);
     }
     if (lane == 0) s_prefix = prefix;
   }
   __syncthreads();
+  const uint32_t prefix = s_prefix;
 
-  uint32_t run = s_prefix + warp_excl + (inc - local);
-  uint32_t o[SCAN_ITEMS];
+  // pass 2: re-read (in may alias out: each thread reads its own elements
+  // before writing them) and write the exclusive prefixes
+  asm volatile("" ::: "memory");
+  uint32_t run = prefix + warp_excl + (inc - local);
+  if (vec) {
+    const uint4* q = reinterpret_cast<const uint4*>(in + base);
+    uint4* w = reinterpret_cast<uint4*>(out + base);
+    const bool vec_out = (((uintptr_t)(out + base)) & 15) == 0;
 #pragma unroll
-  for (int k = 0; k < SCAN_ITEMS; ++k) {
-    o[k] = run;
-    run += v[k];
-  }
-  if (base + SCAN_ITEMS <= n && (((uintptr_t)(out + base)) & 15) == 0) {
-    uint4* q = reinterpret_cast<uint4*>(out + base);
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS / 4; ++k) q[k] = make_uint4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+    for (int k = 0; k < SCAN_ITEMS / 4; ++k) {
+      const uint4 x = q[k];
+      uint4 y;
+      y.x = run;
+      run += x.x;
+      y.y = run;
+      run += x.y;
+      y.z = run;
+      run += x.z;
+      y.w = run;
+      run += x.w;
+      if (vec_out) {
+        w[k] = y;
+      } else {
+        out[base + 4 * k + 0] = y.x;
+        out[base + 4 * k + 1] = y.y;
+        out[base + 4 * k + 2] = y.z;
+        out[base + 4 * k + 3] = y.w;
+      }
+    }
   } else {
-#pragma unroll
     for (int k = 0; k < SCAN_ITEMS; ++k)
-      if (base + k < n) out[base + k] = o[k];
+      if (base + k < n) {
+        const uint32_t x = in[base + k];
+        out[base + k] = run;
+        run += x;
+      }
+  }
+}
+
+// Exclusive scan whose per-tile totals are already known: tile_sum[t] holds
+// the sum of in[t*SCAN_TILE .. (t+1)*SCAN_TILE).  The step's counting kernels
+// accumulate those totals while they count, so each CTA forms its tile's
+// prefix from the totals before it and scans its own tile: one read and one
+// write per element, and no CTA waits on another.
+//
+// Layout: warp w of the CTA owns the contiguous 1024 elements
+// [w*1024, (w+1)*1024) of the tile as 8 rows of 32 uint4; in row k lane l
+// holds elements 4*(32k + l) .. +3, so every load and store instruction of a
+// warp covers 512 contiguous bytes.  Rows are scanned with warp shuffles and
+// carried from row to row; warps are combined through shared memory.
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_with_tile_sums(const uint32_t* __restrict__ in,
+                                                                     uint32_t* __restrict__ out, int64_t n,
+                                                                     const uint32_t* __restrict__ tile_sum) {
+  constexpr int ROWS = SCAN_ITEMS / 4;  // uint4 per lane
+  __shared__ uint32_t s_warp[SCAN_THREADS / 32];
+  __shared__ uint32_t s_pre[SCAN_THREADS / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t tile = blockIdx.x;
+  const int64_t wbase = tile * SCAN_TILE + (int64_t)warp * (32 * SCAN_ITEMS);
+
+  uint32_t pre = 0;
+  for (int64_t t = tid; t < tile; t += SCAN_THREADS) pre += __ldg(tile_sum + t);
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) pre += __shfl_xor_sync(0xffffffffu, pre, d);
+  if (lane == 0) s_pre[warp] = pre;
+
+  const bool full = wbase + 32 * SCAN_ITEMS <= n;
+  uint4 v[ROWS];
+#pragma unroll
+  for (int k = 0; k < ROWS; ++k) {
+    const int64_t e = wbase + 4 * (32 * k + lane);
+    if (full) {
+      v[k] = __ldcs(reinterpret_cast<const uint4*>(in + e));
+    } else {
+      v[k].x = e + 0 < n ? in[e + 0] : 0u;
+      v[k].y = e + 1 < n ? in[e + 1] : 0u;
+      v[k].z = e + 2 < n ? in[e + 2] : 0u;
+      v[k].w = e + 3 < n ? in[e + 3] : 0u;
+    }
+  }
+  // scan row by row inside the warp; `carry` is the warp's running total
+  uint32_t excl[ROWS];
+  uint32_t carry = 0;
+#pragma unroll
+  for (int k = 0; k < ROWS; ++k) {
+    const uint32_t sum = v[k].x + v[k].y + v[k].z + v[k].w;
+    uint32_t inc = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, d);
+      if (lane >= d) inc += t;
+    }
+    excl[k] = carry + inc - sum;
+    carry += __shfl_sync(0xffffffffu, inc, 31);
+  }
+  if (lane == 0) s_warp[warp] = carry;
+  __syncthreads();
+  uint32_t off = 0;
+#pragma unroll
+  for (int w = 0; w < SCAN_THREADS / 32; ++w) off += s_pre[w] + ((w < warp) ? s_warp[w] : 0u);
+#pragma unroll
+  for (int k = 0; k < ROWS; ++k) {
+    const int64_t e = wbase + 4 * (32 * k + lane);
+    uint4 y;
+    y.x = off + excl[k];
+    y.y = y.x + v[k].x;
+    y.z = y.y + v[k].y;
+    y.w = y.z + v[k].z;
+    if (full) {
+      *reinterpret_cast<uint4*>(out + e) = y;
+    } else {
+      if (e + 0 < n) out[e + 0] = y.x;
+      if (e + 1 < n) out[e + 1] = y.y;
+      if (e + 2 < n) out[e + 2] = y.z;
+      if (e + 3 < n) out[e + 3] = y.w;
+    }
   }
 }
 

@@ -23,6 +23,7 @@
 
 #include "ps_device.cuh"
 #include "ps_mesh.cuh"
+#include "ps_scan.cuh"
 
 namespace psb {
 
@@ -67,6 +68,25 @@ __device__ __forceinline__ uint32_t cell_of(T x, T y, T z, const SceneParams<T>&
   return sp.cbase + ((uint32_t)cx * (uint32_t)sp.nb[1] + (uint32_t)cy) * (uint32_t)sp.nb[2] + (uint32_t)cz;
 }
 
+// Cell index of x when the particle was in cell k before: the boundary test
+// settles the usual case (no crossing) exactly; crossings and NaN take the
+// division.  axis_cell is monotonic in x, so B[k] <= x < B[k+1] implies
+// axis_cell(x) == k.
+template <class T>
+__device__ __forceinline__ int32_t axis_cell_near(T x, int32_t k, const T* B, T lo, T iv, int32_t nb) {
+  if (__ldg(B + k) <= x && x < __ldg(B + k + 1)) return k;
+  return axis_cell<T>(x, lo, iv, nb);
+}
+
+template <class T>
+__device__ __forceinline__ uint32_t cell_near(T x, T y, T z, const SceneParams<T>& sp, const T* bounds, int32_t& cx,
+                                              int32_t& cy, int32_t& cz) {
+  cx = axis_cell_near<T>(x, cx, bounds + sp.bnd_base[0], sp.grid_lo[0], sp.interval, sp.nb[0]);
+  cy = axis_cell_near<T>(y, cy, bounds + sp.bnd_base[1], sp.grid_lo[1], sp.interval, sp.nb[1]);
+  cz = axis_cell_near<T>(z, cz, bounds + sp.bnd_base[2], sp.grid_lo[2], sp.interval, sp.nb[2]);
+  return sp.cbase + ((uint32_t)cx * (uint32_t)sp.nb[1] + (uint32_t)cy) * (uint32_t)sp.nb[2] + (uint32_t)cz;
+}
+
 // ---- integrate (PhysicsEngine_kernels.cu:10-16) ------------------------------
 template <class T>
 __device__ __forceinline__ void integrate(vec4_t<T>& P, vec4_t<T>& V, const SceneParams<T>& sp) {
@@ -98,8 +118,10 @@ __device__ __forceinline__ void walls(vec4_t<T>& P, vec4_t<T>& V, const ScenePar
 
 // ---- warp-aggregated cell count --------------------------------------------
 // Lanes hashing to the same cell share one atomicAdd; each receives a
-// distinct slot in [count_before, count_before + peers).
-__device__ __forceinline__ uint32_t count_slot(uint32_t* count, uint32_t c, bool valid) {
+// distinct slot in [count_before, count_before + peers).  The same pass
+// accumulates the per-tile totals of the count array (SCAN_TILE cells per
+// tile) that the step's scan uses in place of a look-back.
+__device__ __forceinline__ uint32_t count_slot(uint32_t* count, uint32_t* tile_sum, uint32_t c, bool valid) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned active = __ballot_sync(0xffffffffu, valid);
   uint32_t slot = 0;
@@ -110,6 +132,15 @@ __device__ __forceinline__ uint32_t count_slot(uint32_t* count, uint32_t c, bool
     if ((int)lane == leader) base = atomicAdd(count + c, (uint32_t)__popc(peers));
     base = __shfl_sync(peers, base, leader);
     slot = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+    const uint32_t t = c / (uint32_t)SCAN_TILE;
+    const int first = __ffs(active) - 1;
+    if (__all_sync(active, t == __shfl_sync(active, t, first))) {
+      // the usual case in sorted order: the whole warp counts into one tile
+      if ((int)lane == first) atomicAdd(tile_sum + t, (uint32_t)__popc(active));
+    } else {
+      const unsigned tpeers = __match_any_sync(active, t);
+      if ((int)lane == __ffs(tpeers) - 1) atomicAdd(tile_sum + t, (uint32_t)__popc(tpeers));
+    }
   }
   return slot;
 }
@@ -131,8 +162,10 @@ struct StepBufs {
   const uint32_t* pbase;  // n_scenes entries
   int32_t n_scenes;
   uint32_t n;             // particles over all scenes
-  uint64_t* scan_scratch; // zeroed by k_begin / k_scatter for the next scan
-  uint32_t scan_words;
+  uint32_t* tile_sum;     // per-tile totals of `count`, cleared by k_scatter
+  uint32_t n_tiles;
+  uint32_t* scell;        // global cell id of each sorted slot (written by k_rank_move)
+  const T* bounds;        // per-scene, per-axis cell boundaries (see SceneParams::bnd_base)
 };
 
 // Container step + hash + count on an integrated state, shared by k_begin and
@@ -157,7 +190,6 @@ __device__ __forceinline__ void finish_integrated(vec4_t<T>& P, vec4_t<T>& V, co
 template <class T, bool MULTI, bool MESH, bool INTEGRATE>
 __global__ void __launch_bounds__(STEP_THREADS) k_begin(StepBufs<T> b, SceneParams<T> sp0, const MeshView* mv) {
   const uint32_t p = blockIdx.x * STEP_THREADS + threadIdx.x;
-  if (p < b.scan_words) b.scan_scratch[p] = 0ull;
   const bool valid = p < b.n;
   uint32_t c = 0;
   if (valid) {
@@ -175,51 +207,124 @@ __global__ void __launch_bounds__(STEP_THREADS) k_begin(StepBufs<T> b, ScenePara
     b.V1[p] = V;
     b.cell[p] = c;
   }
-  const uint32_t s = count_slot(b.count, c, valid);
+  const uint32_t s = count_slot(b.count, b.tile_sum, c, valid);
   if (valid) b.slot[p] = s;
 }
 
+constexpr int MOVE_PER_THREAD = 4;
+
 // tmp[offset[c] + slot] = orig; count[c] = 0 (every non-zero count belongs
-// to a cell some particle hashed to, so this restores an all-zero array).
+// to a cell some particle hashed to, so this restores an all-zero array) and
+// the tile totals are cleared for the next count.
+// MOVE_PER_THREAD particles per thread, strided by the block so that every
+// load instruction stays coalesced; all loads are issued before the stores.
 __global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __restrict__ cell,
                                                           const uint32_t* __restrict__ slot,
                                                           const uint32_t* __restrict__ orig,
                                                           const uint32_t* __restrict__ offset, uint32_t* tmp,
-                                                          uint32_t* count, uint32_t n, uint64_t* scan_scratch,
-                                                          uint32_t scan_words) {
-  const uint32_t p = blockIdx.x * STEP_THREADS + threadIdx.x;
-  if (p < scan_words) scan_scratch[p] = 0ull;
-  if (p >= n) return;
-  const uint32_t c = cell[p];
-  tmp[offset[c] + slot[p]] = orig[p];
-  count[c] = 0u;
+                                                          uint32_t* count, uint32_t n, uint32_t* tile_sum,
+                                                          uint32_t n_tiles) {
+  const uint32_t t = blockIdx.x * STEP_THREADS + threadIdx.x;
+  if (t < n_tiles) tile_sum[t] = 0u;
+  const uint32_t base = blockIdx.x * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
+  uint32_t c[MOVE_PER_THREAD], sl[MOVE_PER_THREAD], o[MOVE_PER_THREAD], off[MOVE_PER_THREAD];
+#pragma unroll
+  for (int k = 0; k < MOVE_PER_THREAD; ++k) {
+    const uint32_t p = base + k * STEP_THREADS;
+    c[k] = p < n ? cell[p] : 0u;
+    sl[k] = p < n ? slot[p] : 0u;
+    o[k] = p < n ? orig[p] : 0u;
+  }
+#pragma unroll
+  for (int k = 0; k < MOVE_PER_THREAD; ++k) off[k] = (base + k * STEP_THREADS) < n ? __ldg(offset + c[k]) : 0u;
+#pragma unroll
+  for (int k = 0; k < MOVE_PER_THREAD; ++k) {
+    if (base + k * STEP_THREADS < n) {
+      tmp[off[k] + sl[k]] = o[k];
+      count[c[k]] = 0u;
+    }
+  }
 }
 
 // Canonical position = offset[c] + #{members of c with a smaller orig id};
 // moves the integrated state (P1, V1) there as (P0, V0) with its orig id.
 template <class T>
 __global__ void __launch_bounds__(STEP_THREADS) k_rank_move(StepBufs<T> b) {
-  const uint32_t p = blockIdx.x * STEP_THREADS + threadIdx.x;
-  if (p >= b.n) return;
-  const uint32_t c = b.cell[p];
-  const uint32_t start = b.offset[c], end = b.offset[c + 1];
-  const uint32_t o = b.tmp[start + b.slot[p]];
-  uint32_t rank = 0;
-  for (uint32_t s = start; s < end; ++s) rank += (b.tmp[s] < o) ? 1u : 0u;
-  const uint32_t d = start + rank;
-  b.P0[d] = b.P1[p];
-  b.V0[d] = b.V1[p];
-  b.orig[d] = o;
+  const uint32_t base = blockIdx.x * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
+  uint32_t c[MOVE_PER_THREAD], sl[MOVE_PER_THREAD];
+#pragma unroll
+  for (int k = 0; k < MOVE_PER_THREAD; ++k) {
+    const uint32_t p = base + k * STEP_THREADS;
+    c[k] = p < b.n ? b.cell[p] : 0u;
+    sl[k] = p < b.n ? b.slot[p] : 0u;
+  }
+#pragma unroll
+  for (int k = 0; k < MOVE_PER_THREAD; ++k) {
+    const uint32_t p = base + k * STEP_THREADS;
+    if (p >= b.n) continue;
+    const uint32_t start = __ldg(b.offset + c[k]), end = __ldg(b.offset + c[k] + 1);
+    const uint32_t o = b.tmp[start + sl[k]];
+    uint32_t rank = 0;
+    for (uint32_t s = start; s < end; ++s) rank += (b.tmp[s] < o) ? 1u : 0u;
+    const uint32_t d = start + rank;
+    b.P0[d] = b.P1[p];
+    b.V0[d] = b.V1[p];
+    b.orig[d] = o;
+    b.scell[d] = c[k];
+  }
 }
 
 // ---- sphere-sphere contacts (ParticleModel_kernels.cu:136-201) --------------
 // One thread per sorted particle; the neighbours are read from the sorted
 // arrays.  For each (dx, dy) column the three z-cells are contiguous in the
 // sorted order, so 9 slot ranges cover the 27 cells, visited x-outer, y,
-// z-inner, members in canonical order.
-template <class T, bool MULTI, bool MESH, bool FUSED>
-__global__ void __launch_bounds__(STEP_THREADS) k_contacts(StepBufs<T> b, SceneParams<T> sp0, const MeshView* mv) {
+// z-inner, members in canonical order.  The 18 range bounds are loaded
+// together before the candidate loop.
+//
+// Candidates far enough apart skip the square root: overlap > 0 holds exactly
+// when sqrt_rn(d2) < s with s = r_i + r_j (rounded); if d2 >= fl(s*s)*(1+2^-20)
+// then d2 > s*s, so sqrt(d2) > s and, rounding being monotonic,
+// sqrt_rn(d2) >= s.  The filter therefore rejects only pairs the exact test
+// rejects, and the result stays bit-identical.
+// Contribution of neighbour j (position Pj) to particle i's velocity.
+template <class T>
+__device__ __forceinline__ void contact_one(const vec4_t<T>* __restrict__ V0, uint32_t j, const vec4_t<T>& P,
+                                            const vec4_t<T>& Vi, const vec4_t<T>& Pj, T k, T e, T& vx, T& vy,
+                                            T& vz) {
   using A = Ar<T>;
+  const T margin = T(1) + T(1.0 / 1048576.0);
+  const T dx = A::sub(P.x, Pj.x), dy = A::sub(P.y, Pj.y), dz = A::sub(P.z, Pj.z);
+  const T d2 = A::fma(dz, dz, A::fma(dy, dy, A::mul(dx, dx)));
+  const T s = A::add(P.w, Pj.w);
+  if (d2 >= A::mul(A::mul(s, s), margin)) return;
+  const T dist = A::sqrt(d2);
+  const T overlap = A::sub(s, dist);
+  if (overlap > T(0)) {
+    const vec4_t<T> Vj = ld4<T>(V0 + j);
+    const T rvx = A::sub(Vi.x, Vj.x), rvy = A::sub(Vi.y, Vj.y), rvz = A::sub(Vi.z, Vj.z);
+    const T rvd = A::fma(rvz, dz, A::fma(rvy, dy, A::mul(rvx, dx)));
+    const T cr = A::div(A::mul(A::mul(A::mul(T(2), Vj.w), rvd), e), A::mul(A::add(Vi.w, Vj.w), d2));
+    const T cs = A::div(A::mul(k, overlap), A::mul(dist, Vi.w));
+    const T f = A::sub(cs, cr);
+    vx = A::fma(f, dx, vx);
+    vy = A::fma(f, dy, vy);
+    vz = A::fma(f, dz, vz);
+  }
+}
+
+// Cell coordinates of a sorted slot from its global cell id.
+template <class T>
+__device__ __forceinline__ void cell_coords(uint32_t c, const SceneParams<T>& sp, int32_t& cx, int32_t& cy,
+                                            int32_t& cz) {
+  const uint32_t local = c - sp.cbase;
+  const uint32_t col = fast_udiv(local, sp.div_nz_m, sp.div_nz_sh1, sp.div_nz_sh2);
+  cz = (int32_t)(local - col * (uint32_t)sp.nb[2]);
+  cx = (int32_t)fast_udiv(col, sp.div_ny_m, sp.div_ny_sh1, sp.div_ny_sh2);
+  cy = (int32_t)(col - (uint32_t)cx * (uint32_t)sp.nb[1]);
+}
+
+template <class T, bool MULTI, bool MESH, bool FUSED>
+__global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 5 : 4) k_contacts(StepBufs<T> b, SceneParams<T> sp0, const MeshView* mv) {
   const uint32_t i = blockIdx.x * STEP_THREADS + threadIdx.x;
   const bool valid = i < b.n;
   uint32_t c = 0;
@@ -228,48 +333,44 @@ __global__ void __launch_bounds__(STEP_THREADS) k_contacts(StepBufs<T> b, SceneP
     vec4_t<T> P = b.P0[i];
     const vec4_t<T> Vi = b.V0[i];
     T vx = Vi.x, vy = Vi.y, vz = Vi.z;
-    const T ri = P.w, mi = Vi.w;
-    const T k = sp.k_spring, e = sp.e_sphere;
     int32_t cx, cy, cz;
-    (void)cell_of<T>(P.x, P.y, P.z, sp, cx, cy, cz);
+    cell_coords<T>(b.scell[i], sp, cx, cy, cz);
     const int32_t nx = sp.nb[0], ny = sp.nb[1], nz = sp.nb[2];
-    const int32_t z0 = cz > 0 ? cz - 1 : 0;
-    const int32_t z1 = cz + 1 < nz ? cz + 1 : nz - 1;
-    for (int32_t bx = cx - 1; bx <= cx + 1; ++bx) {
-      if (bx < 0 || bx >= nx) continue;
-      for (int32_t by = cy - 1; by <= cy + 1; ++by) {
-        if (by < 0 || by >= ny) continue;
-        const uint32_t col = sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz;
-        const uint32_t s0 = __ldg(b.offset + col + (uint32_t)z0);
-        const uint32_t s1 = __ldg(b.offset + col + (uint32_t)z1 + 1u);
-        for (uint32_t j = s0; j < s1; ++j) {
-          if (j == i) continue;
-          const vec4_t<T> Pj = ld4<T>(b.P0 + j);
-          const T dx = A::sub(P.x, Pj.x), dy = A::sub(P.y, Pj.y), dz = A::sub(P.z, Pj.z);
-          const T d2 = A::fma(dz, dz, A::fma(dy, dy, A::mul(dx, dx)));
-          const T dist = A::sqrt(d2);
-          const T overlap = A::sub(A::add(ri, Pj.w), dist);
-          if (overlap > T(0)) {
-            const vec4_t<T> Vj = ld4<T>(b.V0 + j);
-            const T rvx = A::sub(Vi.x, Vj.x), rvy = A::sub(Vi.y, Vj.y), rvz = A::sub(Vi.z, Vj.z);
-            const T rvd = A::fma(rvz, dz, A::fma(rvy, dy, A::mul(rvx, dx)));
-            const T cr = A::div(A::mul(A::mul(A::mul(T(2), Vj.w), rvd), e), A::mul(A::add(mi, Vj.w), d2));
-            const T cs = A::div(A::mul(k, overlap), A::mul(dist, mi));
-            const T f = A::sub(cs, cr);
-            vx = A::fma(f, dx, vx);
-            vy = A::fma(f, dy, vy);
-            vz = A::fma(f, dz, vz);
-          }
-        }
-      }
+    const uint32_t z0 = (uint32_t)(cz > 0 ? cz - 1 : 0);
+    const uint32_t z1 = (uint32_t)(cz + 1 < nz ? cz + 1 : nz - 1) + 1u;
+    uint32_t lo[9], hi[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int32_t bx = cx - 1 + q / 3, by = cy - 1 + q % 3;
+      const bool ok = bx >= 0 && bx < nx && by >= 0 && by < ny;
+      // in-range address even where the column does not exist
+      const uint32_t col = ok ? sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz : sp.cbase;
+      lo[q] = ok ? __ldg(b.offset + col + z0) : 0u;
+      hi[q] = ok ? __ldg(b.offset + col + z1) : 0u;
     }
+    // visit the nine ranges in canonical order
+    const T ks = sp.k_spring, es = sp.e_sphere;
+#pragma unroll
+    for (int q = 0; q < 9; ++q)
+      for (uint32_t j = lo[q]; j < hi[q]; ++j) {
+        if (j == i) continue;
+        contact_one<T>(b.V0, j, P, Vi, ld4<T>(b.P0 + j), ks, es, vx, vy, vz);
+      }
     vec4_t<T> V = Vi;
     V.x = vx;
     V.y = vy;
     V.z = vz;
     if (FUSED) {
       integrate<T>(P, V, sp);
-      finish_integrated<T, MESH>(P, V, sp, mv, b.err, c);
+      if constexpr (MESH) {
+        if (sp.mesh_tris > 0)
+          mesh_contacts<T>(P, V, sp, *mv, b.err);
+        else
+          walls<T>(P, V, sp);
+      } else {
+        walls<T>(P, V, sp);
+      }
+      c = cell_near<T>(P.x, P.y, P.z, sp, b.bounds, cx, cy, cz);
       b.P1[i] = P;
       b.V1[i] = V;
       b.cell[i] = c;
@@ -278,7 +379,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_contacts(StepBufs<T> b, SceneP
     }
   }
   if (FUSED) {
-    const uint32_t s = count_slot(b.count, c, valid);
+    const uint32_t s = count_slot(b.count, b.tile_sum, c, valid);
     if (valid) b.slot[i] = s;
   }
 }

@@ -1,0 +1,71 @@
+"""Generate tests/golden/ref_cuda_*.npz from the reference's own CUDA simulator.
+
+Needs a GPU and oracle/_ref/libref_cuda.so (the reference CUDA sources
+compiled for sm_100a by `make -C oracle ref`):
+
+    python tests/golden/make_golden_cuda.py OUTDIR
+
+For two small box scenes whose dynamics stay tame (a jittered lattice and a
+soft contact-rich pile), it records after several step counts the
+reference's bucket arrays (per-cell counts, exclusive offsets, particle
+index list) and its particle states.  The CPU tests pin the oracle's CUDA
+scheme to these.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "particle-stabilizer_b200", "python"))
+
+from oracle import ps_oracle as O  # noqa: E402
+from psb200 import scenes  # noqa: E402
+
+STEPS = (1, 5, 30)
+
+
+def record(sc, name, outdir):
+    r = O.ref_cuda()
+    h = r.create(sc)
+    nb = (C.c_int32 * 3)()
+    iv = C.c_double()
+    lo = (C.c_double * 3)()
+    r.lib.refc_get_grid(h, nb, C.byref(iv), lo)
+    n_cells = nb[0] * nb[1] * nb[2]
+    counts, offsets, buckets, states = [], [], [], []
+    done = 0
+    for s in STEPS:
+        r.step(h, s - done)
+        done = s
+        c = np.empty(n_cells, dtype=np.uint32)
+        o = np.empty(n_cells, dtype=np.uint32)
+        b = np.empty(sc.n, dtype=np.int64)
+        r.lib.refc_get_buckets(h, C.c_void_p(c.ctypes.data), C.c_void_p(o.ctypes.data), C.c_void_p(b.ctypes.data))
+        counts.append(c)
+        offsets.append(o)
+        buckets.append(b)
+        states.append(r.state(h, sc.n))
+    r.destroy(h)
+    np.savez_compressed(os.path.join(outdir, f"ref_cuda_{name}.npz"), steps=np.array(STEPS), init=sc.state,
+                        box=np.array([sc.box_min, sc.box_max]), e_wall=np.array(sc.e_wall), k=sc.k_spring,
+                        es=sc.e_sphere, dt=sc.dt, nb=np.array(list(nb)), interval=iv.value,
+                        counts=np.stack(counts), offsets=np.stack(offsets), bucket=np.stack(buckets),
+                        out=np.stack(states))
+
+
+def main():
+    outdir = sys.argv[1] if len(sys.argv) > 1 else HERE
+    os.makedirs(outdir, exist_ok=True)
+    record(scenes.lattice_c1(side=8), "lattice", outdir)
+    record(scenes.pile(600, seed=51, k_spring=1.0), "pile", outdir)
+    print("reference CUDA fixtures written to", outdir)
+
+
+if __name__ == "__main__":
+    main()

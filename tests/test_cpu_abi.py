@@ -1,0 +1,113 @@
+"""The C ABI library without a GPU: exports, error behaviour, file formats.
+
+Every function declared in include/*.h must be exported by
+libparticle_stabilizer_cuda.so.  The CSV and OBJ readers/writer run on the
+host and are compared with what the reference's own code produced
+(tests/golden/ref_io.npz, from tests/golden/make_golden.py).
+"""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import psb200
+from conftest import GOLDEN, ROOT, gpu_available
+
+
+def declared_functions():
+    names = set()
+    for h in ("particle_stabilizer_b200.h", "ps_runsimulate.hpp"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        for m in re.finditer(r"\b(ps_[a-z0-9_]+|runSimulateCUDA)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert "ps_create" in names and "runSimulateCUDA" in names and len(names) >= 20
+    lib = psb200.lib()
+    for n in names:
+        getattr(lib, n)  # raises AttributeError if missing
+    out = subprocess.run(["nm", "-D", "--defined-only", psb200.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    assert set(names) <= exported
+    assert set(psb200.EXPORTED) <= exported
+    # nothing else leaks out of the library
+    assert all(e.startswith("ps_") or e == "runSimulateCUDA" for e in exported)
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU error path")
+def test_create_without_gpu_is_a_clean_error():
+    sc = psb200.scenes.pile(16)
+    with pytest.raises(psb200.PSError) as e:
+        psb200.Simulation(sc)
+    assert "ps_create" in str(e.value)
+    assert psb200.lib().ps_last_error()  # message recorded
+
+
+def test_bad_arguments_rejected_before_any_cuda_call():
+    h = C.c_void_p()
+    assert psb200.lib().ps_create(None, 1, 0, 0, C.byref(h)) == -1
+    assert psb200.lib().ps_step(None, 1) == -1
+    assert psb200.lib().ps_destroy(None) == 0
+    assert psb200.exclusive_scan_scratch_bytes(0) == 8
+
+
+def test_read_csv_matches_reference_reader():
+    g = np.load(os.path.join(GOLDEN, "ref_io.npz"))
+    got = psb200.read_csv(os.path.join(GOLDEN, "io_cases.csv"), tuple(g["csv_velocity"]), float(g["csv_density"]))
+    assert np.array_equal(got, g["csv_state"])
+
+
+def test_write_csv_matches_reference_writer(tmp_path):
+    g = np.load(os.path.join(GOLDEN, "ref_io.npz"))
+    out = tmp_path / "sub" / "w.csv"  # the writer creates missing directories, as the reference does
+    psb200.write_csv(str(out), g["write_state"])
+    assert out.read_text() == str(g["write_text"])
+
+
+def test_read_obj_matches_reference_deindexing():
+    g = np.load(os.path.join(GOLDEN, "ref_io.npz"))
+    got = psb200.read_obj(os.path.join(GOLDEN, "cube.obj"))
+    assert np.array_equal(got, g["obj_tri"])
+
+
+def test_io_errors(tmp_path):
+    with pytest.raises(psb200.PSError, match="Could not open"):
+        psb200.read_csv(str(tmp_path / "missing.csv"))
+    bad = tmp_path / "bad.csv"
+    bad.write_text("x,y,z,r\n1,2,abc,4\n")
+    with pytest.raises(psb200.PSError, match="bad number"):
+        psb200.read_csv(str(bad))
+    with pytest.raises(psb200.PSError, match="Unable to open"):
+        psb200.read_obj(str(tmp_path / "missing.obj"))
+    obj = tmp_path / "bad.obj"
+    obj.write_text("v 0 0 0\nf 1 2 3\n")
+    with pytest.raises(psb200.PSError, match="out of range"):
+        psb200.read_obj(str(obj))
+
+
+def test_obj_roundtrip_of_the_funnel(tmp_path):
+    tri = psb200.scenes.funnel_triangles(n_seg=24, n_cone=4, n_cyl=2, n_ring=2)
+    p = tmp_path / "f.obj"
+    psb200.scenes.write_obj(str(p), tri)
+    assert np.array_equal(psb200.read_obj(str(p)), tri)
+
+
+def test_cli_help_and_missing_input(tmp_path):
+    exe = psb200.CLI_PATH
+    r = subprocess.run([exe, "-h"], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 0 and "--coeff-of-restitution-wall" in r.stdout
+    lib = os.path.dirname(psb200.LIB_PATH)
+    r = subprocess.run([exe, "--lib", os.path.join(lib, "libparticle_stabilizer_cuda.so"), "missing.csv", "--cuda"],
+                       capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode != 0 and "Could not open file" in (r.stderr + r.stdout)
+    r = subprocess.run([exe, "--lib", str(tmp_path / "nolib.so"), "x.csv"], capture_output=True, text=True,
+                       cwd=tmp_path)
+    assert r.returncode != 0 and "Cannot open library" in r.stderr
