@@ -161,6 +161,29 @@ int ps_profile_steps(ps_sim* sim, int64_t n_steps, double* kernel_ms, int64_t* k
 
 int ps_destroy(ps_sim* sim);
 
+/* ---- differentiation (no counterpart in the reference) -------------------
+ * Gradients of a loss of the final state with respect to the spring
+ * coefficient, the sphere restitution, the six wall restitutions and the
+ * initial state, for box-container scenes.  Two calls:
+ *   ps_forward_checkpointed  advances n_steps from the current state,
+ *                            keeping a device checkpoint every
+ *                            `checkpoint_every` steps;
+ *   ps_backward              given dL/d(final state), re-runs each block of
+ *                            steps from its checkpoint and sweeps the adjoint
+ *                            of contacts, walls and integration backwards.
+ * Wall clamps and contact activation are taken as fixed events of the
+ * forward values.  dl_dstate and dl_dstate0 are n_total x 6 doubles
+ * (dL/dx, dL/dy, dL/dz, dL/dvx, dL/dvy, dL/dvz) in original particle order;
+ * grads has one entry per scene.  After ps_backward the state is the final
+ * state again. */
+typedef struct ps_grad {
+  double k_spring;
+  double e_sphere;
+  double e_wall[6];          /* PS_ZMIN..PS_YMAX */
+} ps_grad;
+int ps_forward_checkpointed(ps_sim* sim, int64_t n_steps, int64_t checkpoint_every);
+int ps_backward(ps_sim* sim, const double* dl_dstate, ps_grad* grads, double* dl_dstate0);
+
 /* runSimulateCUDA with POD arguments: create, upload, max_steps steps,
  * download, destroy.  aos_out may alias aos_in. */
 int ps_simulate(const ps_scene_desc* scene, const double* aos_in, double* aos_out, int64_t max_steps,

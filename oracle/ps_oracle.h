@@ -122,6 +122,13 @@ void or_mesh_f32(float* p, int64_t n, const double* tri, int64_t n_tri, double e
                  int32_t edge_quirk);
 int32_t or_run_f32(float* p, int64_t n, const or_params* prm, int64_t steps);
 
+/* ---- forward-mode reference gradients (FP64, box container) ----------- */
+/* Values as or_run_f64; dparam: nd x 8 parameter tangents (k_spring,
+ * e_sphere, e_wall[6]); dstate: nd x n x 6 state tangents (x, y, z, vx, vy,
+ * vz), updated in place.  Returns 0, or negative on bad input.            */
+int32_t or_run_dual_f64(double* p, int64_t n, const or_params* prm, int64_t steps, int32_t nd,
+                        const double* dparam, double* dstate);
+
 /* ---- statistics (ParticleStatisticsCUDA.cpp:11-62) -------------------- */
 typedef struct {
   double kinetic_energy;

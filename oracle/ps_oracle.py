@@ -123,6 +123,23 @@ def run(scene: Scene, steps: int, precision: str = "f64", cpu_semantics: bool = 
     return st
 
 
+def run_dual(scene, steps: int, dparam: np.ndarray, dstate0: np.ndarray):
+    """Forward-mode FP64 run: returns (state, tangents) with tangents of
+    shape (nd, n, 6) for the parameter tangents dparam (nd, 8) = (k_spring,
+    e_sphere, e_wall[6]) and initial state tangents dstate0 (nd, n, 6)."""
+    prm, keep = params_for(scene)
+    st = np.ascontiguousarray(scene.state, dtype=np.float64).copy()
+    dp = np.ascontiguousarray(dparam, dtype=np.float64)
+    ds = np.ascontiguousarray(dstate0, dtype=np.float64).copy()
+    lib().or_run_dual_f64.restype = C.c_int32
+    rc = lib().or_run_dual_f64(_p(st), C.c_int64(scene.n), C.byref(prm), C.c_int64(steps), C.c_int32(dp.shape[0]),
+                               _p(dp), _p(ds))
+    del keep
+    if rc != 0:
+        raise RuntimeError(f"oracle dual run failed: {rc}")
+    return st, ds
+
+
 def cell_ids(state: np.ndarray, grid: OrGrid, clamp: bool = True) -> np.ndarray:
     st = np.ascontiguousarray(state)
     out = np.empty(st.shape[0], dtype=np.int64)

@@ -1,0 +1,221 @@
+// ps_adjoint.cuh — reverse-mode adjoint of the DEM step (box container).
+//
+// Forward step (per particle i, the CUDA scheme of PhysicsEngineCUDA.cpp:38-42):
+//   x' = x + v dt,  v' = v + g dt                       (integrate)
+//   per axis: clamp to the walls, v <- -v e              (walls, events)
+//   v''' = v'' + sum_j f_ij d_ij,  x''' = x''            (Jacobi contacts)
+//   d = x_i - x_j, L = |d|, ov = r_i + r_j - L > 0,
+//   f = k ov / (L m_i) - B (u.d) / L^2,  B = 2 m_j e / (m_i + m_j),  u = v_i - v_j
+//
+// Reverse sweep of one step, given the adjoints (xbar, vbar) of its output:
+//   k_adj_contacts   (sorted order, gather): for each particle, the terms of
+//                    the pairs where it receives and the pairs where it is the
+//                    source (pairs are symmetric), so no atomics; per-particle
+//                    partials of dL/dk and dL/de_sphere.
+//   k_adj_walls_integrate (original order): through the walls (clamp events
+//                    recomputed from the recorded step input) and the
+//                    integrate; per-particle partials of dL/de_wall.
+// Wall clamps and contact activation are piecewise events taken from the
+// forward values; radii and masses are constants.
+#pragma once
+
+#include "ps_step_kernels.cuh"
+
+namespace psb {
+
+enum : int { ADJ_K = 0, ADJ_E = 1, ADJ_WALL = 2 };  // acc layout: k, e_sphere, e_wall[6] (zMin..yMax)
+constexpr int ADJ_NACC = 8;
+
+template <class T>
+struct AdjBufs {
+  const vec4_t<T>* tape;  // step input, original order: [2*o] = (x, r), [2*o+1] = (v, m)
+  T* ax;                  // adjoint of positions (3 per particle, original order)
+  T* av;                  // adjoint of velocities
+  T* ax2;                 // output of k_adj_contacts
+  T* av2;
+  double* acc;            // ADJ_NACC per particle, original order, accumulated over steps
+};
+
+// Terms of one active pair for the receiver r and the source s:
+// c_r = f d; g = adjoint of v_r's output.  Returns the adjoint of d (dd),
+// of u (du) and the parameter partials.
+template <class T>
+__device__ __forceinline__ void pair_adjoint(T dx, T dy, T dz, T ux, T uy, T uz, T R, T mr, T ms, T k, T e, T gx,
+                                             T gy, T gz, T& ddx, T& ddy, T& ddz, T& dux, T& duy, T& duz,
+                                             double& dk, double& de) {
+  const T L2 = dx * dx + dy * dy + dz * dz;
+  const T L = sqrt(L2);
+  const T ov = R - L;
+  const T Bc = T(2) * ms * e / (mr + ms);
+  const T ud = ux * dx + uy * dy + uz * dz;
+  const T f = k * ov / (L * mr) - Bc * ud / L2;
+  const T fbar = gx * dx + gy * dy + gz * dz;
+  dk += (double)(fbar * ov / (L * mr));
+  de += (double)(fbar * (-(T(2) * ms * ud) / ((mr + ms) * L2)));
+  const T fL = -k * R / (L2 * mr) + T(2) * Bc * ud / (L2 * L);
+  const T Lb = fbar * fL / L;
+  const T udb = -fbar * Bc / L2;
+  ddx = f * gx + Lb * dx + udb * ux;
+  ddy = f * gy + Lb * dy + udb * uy;
+  ddz = f * gz + Lb * dz + udb * uz;
+  dux = udb * dx;
+  duy = udb * dy;
+  duz = udb * dz;
+}
+
+// Same activation test as the forward contact kernel (contact_one).
+template <class T>
+__device__ __forceinline__ bool pair_active(const vec4_t<T>& P, const vec4_t<T>& Pj) {
+  using A = Ar<T>;
+  const T margin = T(1) + T(1.0 / 1048576.0);
+  const T dx = A::sub(P.x, Pj.x), dy = A::sub(P.y, Pj.y), dz = A::sub(P.z, Pj.z);
+  const T d2 = A::fma(dz, dz, A::fma(dy, dy, A::mul(dx, dx)));
+  const T s = A::add(P.w, Pj.w);
+  if (d2 >= A::mul(A::mul(s, s), margin)) return false;
+  return A::sub(s, A::sqrt(d2)) > T(0);
+}
+
+template <class T, bool MULTI>
+__global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, AdjBufs<T> a, SceneParams<T> sp0) {
+  const uint32_t i = blockIdx.x * STEP_THREADS + threadIdx.x;
+  if (i >= b.n) return;
+  const SceneParams<T>& sp = scene_of<T, MULTI>(i, sp0, b.scenes, b.pbase, b.n_scenes);
+  const vec4_t<T> P = b.P0[i];
+  const vec4_t<T> V = b.V0[i];
+  const uint32_t oi = b.orig[i];
+  const T gx = a.av[3 * oi], gy = a.av[3 * oi + 1], gz = a.av[3 * oi + 2];
+  T xb0 = a.ax[3 * oi], xb1 = a.ax[3 * oi + 1], xb2 = a.ax[3 * oi + 2];
+  T vb0 = gx, vb1 = gy, vb2 = gz;
+  double dk = 0.0, de = 0.0;
+  int32_t cx, cy, cz;
+  cell_coords<T>(b.scell[i], sp, cx, cy, cz);
+  const int32_t nx = sp.nb[0], ny = sp.nb[1], nz = sp.nb[2];
+  const uint32_t z0 = (uint32_t)(cz > 0 ? cz - 1 : 0);
+  const uint32_t z1 = (uint32_t)(cz + 1 < nz ? cz + 1 : nz - 1) + 1u;
+  const T k = sp.k_spring, e = sp.e_sphere;
+  for (int q = 0; q < 9; ++q) {
+    const int32_t bx = cx - 1 + q / 3, by = cy - 1 + q % 3;
+    if (bx < 0 || bx >= nx || by < 0 || by >= ny) continue;
+    const uint32_t col = sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz;
+    const uint32_t j0 = b.offset[col + z0], j1 = b.offset[col + z1];
+    for (uint32_t j = j0; j < j1; ++j) {
+      if (j == i) continue;
+      const vec4_t<T> Pj = b.P0[j];
+      if (!pair_active<T>(P, Pj)) continue;
+      const vec4_t<T> Vj = b.V0[j];
+      const uint32_t oj = b.orig[j];
+      const T dx = P.x - Pj.x, dy = P.y - Pj.y, dz = P.z - Pj.z;
+      const T ux = V.x - Vj.x, uy = V.y - Vj.y, uz = V.z - Vj.z;
+      const T R = P.w + Pj.w;
+      T ddx, ddy, ddz, dux, duy, duz;
+      // i receives from j
+      pair_adjoint<T>(dx, dy, dz, ux, uy, uz, R, V.w, Vj.w, k, e, gx, gy, gz, ddx, ddy, ddz, dux, duy, duz, dk, de);
+      xb0 += ddx;
+      xb1 += ddy;
+      xb2 += ddz;
+      vb0 += dux;
+      vb1 += duy;
+      vb2 += duz;
+      // j receives from i: i enters as the source (d and u change sign)
+      double dk2 = 0.0, de2 = 0.0;
+      const T hx = a.av[3 * oj], hy = a.av[3 * oj + 1], hz = a.av[3 * oj + 2];
+      pair_adjoint<T>(-dx, -dy, -dz, -ux, -uy, -uz, R, Vj.w, V.w, k, e, hx, hy, hz, ddx, ddy, ddz, dux, duy, duz, dk2,
+                      de2);
+      xb0 -= ddx;
+      xb1 -= ddy;
+      xb2 -= ddz;
+      vb0 -= dux;
+      vb1 -= duy;
+      vb2 -= duz;
+    }
+  }
+  a.ax2[3 * oi] = xb0;
+  a.ax2[3 * oi + 1] = xb1;
+  a.ax2[3 * oi + 2] = xb2;
+  a.av2[3 * oi] = vb0;
+  a.av2[3 * oi + 1] = vb1;
+  a.av2[3 * oi + 2] = vb2;
+  a.acc[ADJ_NACC * oi + ADJ_K] += dk;
+  a.acc[ADJ_NACC * oi + ADJ_E] += de;
+}
+
+// Walls + integrate adjoint, original order.  The step input (x, v) comes
+// from the tape; x' and v' and the clamp events are recomputed from it with
+// the forward's operations.
+template <class T, bool MULTI>
+__global__ void __launch_bounds__(STEP_THREADS) k_adj_walls_integrate(StepBufs<T> b, AdjBufs<T> a,
+                                                                      SceneParams<T> sp0) {
+  const uint32_t o = blockIdx.x * STEP_THREADS + threadIdx.x;
+  if (o >= b.n) return;
+  const SceneParams<T>& sp = scene_of<T, MULTI>(o, sp0, b.scenes, b.pbase, b.n_scenes);
+  vec4_t<T> P = a.tape[2 * (size_t)o];
+  vec4_t<T> V = a.tape[2 * (size_t)o + 1];
+  integrate<T>(P, V, sp);  // x', v'
+  using A = Ar<T>;
+  const T r = P.w;
+  const T xs[3] = {P.x, P.y, P.z}, vs[3] = {V.x, V.y, V.z};
+  const int lo_idx[3] = {PS_XMIN, PS_YMIN, PS_ZMIN}, hi_idx[3] = {PS_XMAX, PS_YMAX, PS_ZMAX};
+  double* acc = a.acc + ADJ_NACC * (size_t)o;
+  for (int ax = 0; ax < 3; ++ax) {
+    const bool lo_hit = A::sub(xs[ax], r) < sp.box_lo[ax];
+    const bool hi_hit = A::add(xs[ax], r) > sp.box_hi[ax];
+    T xb = a.ax2[3 * o + ax], vb = a.av2[3 * o + ax];
+    const T v1 = lo_hit ? A::mul(-vs[ax], sp.e_lo[ax]) : vs[ax];  // velocity after the min clamp
+    if (hi_hit) {
+      acc[ADJ_WALL + hi_idx[ax]] += (double)(-v1 * vb);
+      vb = -sp.e_hi[ax] * vb;
+      xb = T(0);
+    }
+    if (lo_hit) {
+      acc[ADJ_WALL + lo_idx[ax]] += (double)(-vs[ax] * vb);
+      vb = -sp.e_lo[ax] * vb;
+      xb = T(0);
+    }
+    // integrate: x' = x + v dt, v' = v + g dt
+    a.ax[3 * o + ax] = xb;
+    a.av[3 * o + ax] = vb + sp.dt * xb;
+  }
+}
+
+// Gather the at-rest state (P0, V1) into the tape row in original order.
+template <class T>
+__global__ void k_tape_write(StepBufs<T> b, vec4_t<T>* row) {
+  const uint32_t p = blockIdx.x * STEP_THREADS + threadIdx.x;
+  if (p >= b.n) return;
+  const uint32_t o = b.orig[p];
+  row[2 * (size_t)o] = b.P0[p];
+  row[2 * (size_t)o + 1] = b.V1[p];
+}
+
+// Put a tape row back as the at-rest state in original order (orig = id).
+template <class T>
+__global__ void k_tape_read(StepBufs<T> b, const vec4_t<T>* row) {
+  const uint32_t o = blockIdx.x * STEP_THREADS + threadIdx.x;
+  if (o >= b.n) return;
+  b.P0[o] = row[2 * (size_t)o];
+  b.V1[o] = row[2 * (size_t)o + 1];
+  b.orig[o] = o;
+}
+
+// Per-scene sums of the per-particle parameter partials, in a fixed order.
+__global__ void k_adj_reduce(const double* acc, const uint32_t* pbase, int n_scenes, uint32_t n, double* out) {
+  const int s = blockIdx.x;
+  if (s >= n_scenes) return;
+  const uint32_t p0 = pbase[s], p1 = s + 1 < n_scenes ? pbase[s + 1] : n;
+  __shared__ double red[ADJ_NACC][128];
+  double loc[ADJ_NACC];
+  for (int c = 0; c < ADJ_NACC; ++c) loc[c] = 0.0;
+  for (uint32_t p = p0 + threadIdx.x; p < p1; p += blockDim.x)
+    for (int c = 0; c < ADJ_NACC; ++c) loc[c] += acc[ADJ_NACC * (size_t)p + c];
+  for (int c = 0; c < ADJ_NACC; ++c) red[c][threadIdx.x] = loc[c];
+  __syncthreads();
+  for (int w = 64; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int c = 0; c < ADJ_NACC; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < ADJ_NACC; ++c) out[ADJ_NACC * s + c] = red[c][0];
+}
+
+}  // namespace psb

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "particle_stabilizer_b200.h"
+#include "ps_adjoint.cuh"
 #include "ps_scan.cuh"
 #include "ps_stats.cuh"
 #include "ps_step_kernels.cuh"
@@ -114,6 +115,11 @@ struct ps_sim {
   std::map<int32_t, void*> checkpoints;  // slot -> device copy of (P0, V1, orig)
   cudaAccessPolicyWindow l2_window{};     // count + offset arrays kept in L2
   bool l2_window_on = false;
+  // differentiation
+  int64_t fwd_steps = 0, fwd_every = 0;   // last ps_forward_checkpointed
+  std::vector<void*> fwd_ckpt;            // state at the start of each block, + final state last
+  void* adj_arena = nullptr;              // tape, adjoint arrays, partials
+  size_t adj_bytes = 0;
 };
 
 namespace {
@@ -616,7 +622,7 @@ int size_grids(ps_sim* s, const double* aos) {
         phi[a] = std::max(phi[a], q[a]);
       }
     }
-    if (d.tri != nullptr && d.n_tri > 0) {
+    if (!s->tris[sc].empty()) {  // ps_create keeps the soup in s->tris (desc.tri is cleared)
       const std::vector<double>& soup = s->tris[sc];
       for (int a = 0; a < 3; ++a) {
         g.min[a] = INFINITY;
@@ -724,6 +730,9 @@ int size_grids(ps_sim* s, const double* aos) {
 }
 
 void free_sim(ps_sim* s) {
+  for (void* p : s->fwd_ckpt) cudaFree(p);
+  s->fwd_ckpt.clear();
+  cudaFree(s->adj_arena);
   if (s->l2_window_on) {
     cudaStreamAttrValue v{};
     v.accessPolicyWindow.num_bytes = 0;
@@ -746,6 +755,140 @@ void free_sim(ps_sim* s) {
   cudaFree(s->d_bin_tri);
   cudaFree(s->d_mesh_view);
   if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+// ---- differentiation -----------------------------------------------------------
+size_t state_bytes(const ps_sim* s) { return (size_t)(s->precision == PS_FP32 ? 16 : 32) * (size_t)s->n_total; }
+
+int save_state(ps_sim* s, void*& buf) {
+  const size_t vb = state_bytes(s), ob = 4 * (size_t)s->n_total;
+  if (buf == nullptr) PS_CUDA(cudaMalloc(&buf, std::max<size_t>(2 * vb + ob, 16)));
+  char* p = static_cast<char*>(buf);
+  PS_CUDA(cudaMemcpyAsync(p, s->P0, vb, cudaMemcpyDeviceToDevice, s->stream));
+  PS_CUDA(cudaMemcpyAsync(p + vb, s->V1, vb, cudaMemcpyDeviceToDevice, s->stream));
+  PS_CUDA(cudaMemcpyAsync(p + 2 * vb, s->orig, ob, cudaMemcpyDeviceToDevice, s->stream));
+  return PS_OK;
+}
+
+int load_state(ps_sim* s, const void* buf) {
+  const size_t vb = state_bytes(s), ob = 4 * (size_t)s->n_total;
+  const char* p = static_cast<const char*>(buf);
+  PS_CUDA(cudaMemcpyAsync(s->P0, p, vb, cudaMemcpyDeviceToDevice, s->stream));
+  PS_CUDA(cudaMemcpyAsync(s->V1, p + vb, vb, cudaMemcpyDeviceToDevice, s->stream));
+  PS_CUDA(cudaMemcpyAsync(s->orig, p + 2 * vb, ob, cudaMemcpyDeviceToDevice, s->stream));
+  s->grid_valid = false;
+  return PS_OK;
+}
+
+// integrate + walls + grid of the at-rest state, leaving the sorted post-wall
+// state in (P0, V0) for the contact adjoint (the first half of a step)
+template <class T, bool MULTI>
+void enqueue_prepare(ps_sim* s) {
+  const StepBufs<T> b = bufs<T>(s);
+  const SceneParams<T> sp0 = params<T>(s)[0];
+  const unsigned gp = blocks_for(s->n_total);
+  cudaStream_t st = s->stream;
+  k_begin<T, MULTI, false, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+  k_scan_with_tile_sums<<<(unsigned)scan_num_tiles(n_scan(s)), SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s),
+                                                                                     s->tile_sum);
+  k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
+                                                                       s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
+  k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
+}
+
+template <class T>
+__global__ void k_adj_upload(const double* __restrict__ g, T* ax, T* av, uint32_t n) {
+  const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  for (int c = 0; c < 3; ++c) {
+    ax[3 * o + c] = (T)g[6 * (size_t)o + c];
+    av[3 * o + c] = (T)g[6 * (size_t)o + 3 + c];
+  }
+}
+
+template <class T>
+__global__ void k_adj_download(const T* ax, const T* av, double* __restrict__ g, uint32_t n) {
+  const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  for (int c = 0; c < 3; ++c) {
+    g[6 * (size_t)o + c] = (double)ax[3 * o + c];
+    g[6 * (size_t)o + 3 + c] = (double)av[3 * o + c];
+  }
+}
+
+template <class T, bool MULTI>
+int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl_dstate0) {
+  const int64_t n = s->n_total, K = s->fwd_every;
+  const size_t tape_b = align_up(2 * sizeof(vec4_t<T>) * (size_t)n * (size_t)K, 256);
+  const size_t adj_b = align_up(3 * sizeof(T) * (size_t)n, 256);
+  const size_t acc_b = align_up(ADJ_NACC * sizeof(double) * (size_t)n, 256);
+  const size_t io_b = align_up(6 * sizeof(double) * (size_t)n, 256);
+  const size_t red_b = align_up(ADJ_NACC * sizeof(double) * (size_t)s->n_scenes, 256);
+  const size_t need = tape_b + 4 * adj_b + acc_b + io_b + red_b;
+  if (s->adj_bytes < need) {
+    cudaFree(s->adj_arena);
+    s->adj_arena = nullptr;
+    s->adj_bytes = 0;
+    PS_CUDA(cudaMalloc(&s->adj_arena, need));
+    s->adj_bytes = need;
+  }
+  char* p = static_cast<char*>(s->adj_arena);
+  vec4_t<T>* tape = reinterpret_cast<vec4_t<T>*>(p);
+  p += tape_b;
+  AdjBufs<T> a;
+  a.tape = tape;
+  a.ax = reinterpret_cast<T*>(p); p += adj_b;
+  a.av = reinterpret_cast<T*>(p); p += adj_b;
+  a.ax2 = reinterpret_cast<T*>(p); p += adj_b;
+  a.av2 = reinterpret_cast<T*>(p); p += adj_b;
+  a.acc = reinterpret_cast<double*>(p); p += acc_b;
+  double* io = reinterpret_cast<double*>(p); p += io_b;
+  double* red = reinterpret_cast<double*>(p);
+  cudaStream_t st = s->stream;
+  const unsigned gp = blocks_for(n);
+  PS_CUDA(cudaMemcpyAsync(io, dl_dstate, 6 * sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, st));
+  k_adj_upload<T><<<gp, STEP_THREADS, 0, st>>>(io, a.ax, a.av, (uint32_t)n);
+  PS_CUDA(cudaMemsetAsync(a.acc, 0, acc_b, st));
+  const SceneParams<T> sp0 = params<T>(s)[0];
+  const int64_t n_blocks = (s->fwd_steps + K - 1) / K;
+  for (int64_t blk = n_blocks - 1; blk >= 0; --blk) {
+    const int64_t kb = std::min(K, s->fwd_steps - blk * K);
+    int rc = load_state(s, s->fwd_ckpt[(size_t)blk]);
+    if (rc != PS_OK) return rc;
+    for (int64_t t = 0; t < kb; ++t) {  // recompute the block, recording each step's input
+      StepBufs<T> b = bufs<T>(s);
+      k_tape_write<T><<<gp, STEP_THREADS, 0, st>>>(b, tape + 2 * (size_t)n * (size_t)t);
+      if (t + 1 < kb) {
+        rc = ps_step(s, 1);
+        if (rc != PS_OK) return rc;
+      }
+    }
+    for (int64_t t = kb - 1; t >= 0; --t) {
+      StepBufs<T> b = bufs<T>(s);
+      a.tape = tape + 2 * (size_t)n * (size_t)t;
+      k_tape_read<T><<<gp, STEP_THREADS, 0, st>>>(b, a.tape);
+      enqueue_prepare<T, MULTI>(s);
+      k_adj_contacts<T, MULTI><<<gp, STEP_THREADS, 0, st>>>(b, a, sp0);
+      k_adj_walls_integrate<T, MULTI><<<gp, STEP_THREADS, 0, st>>>(b, a, sp0);
+      PS_CUDA(cudaGetLastError());
+    }
+  }
+  k_adj_reduce<<<s->n_scenes, 128, 0, st>>>(a.acc, s->d_pbase, s->n_scenes, (uint32_t)n, red);
+  std::vector<double> h((size_t)ADJ_NACC * s->n_scenes);
+  PS_CUDA(cudaMemcpyAsync(h.data(), red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+  if (dl_dstate0 != nullptr) {
+    k_adj_download<T><<<gp, STEP_THREADS, 0, st>>>(a.ax, a.av, io, (uint32_t)n);
+    PS_CUDA(cudaMemcpyAsync(dl_dstate0, io, 6 * sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, st));
+  }
+  PS_CUDA(cudaStreamSynchronize(st));
+  for (int sc = 0; sc < s->n_scenes; ++sc) {
+    grads[sc].k_spring = h[ADJ_NACC * sc + ADJ_K];
+    grads[sc].e_sphere = h[ADJ_NACC * sc + ADJ_E];
+    for (int w = 0; w < 6; ++w) grads[sc].e_wall[w] = h[ADJ_NACC * sc + ADJ_WALL + w];
+  }
+  const int rc = load_state(s, s->fwd_ckpt.back());  // leave the final state in place
+  if (rc != PS_OK) return rc;
+  return check_device_error(s);
 }
 
 }  // namespace
@@ -991,6 +1134,37 @@ extern "C" int ps_profile_steps(ps_sim* s, int64_t n_steps, double* kernel_ms, i
   if (le != cudaSuccess) return fail(PS_ERR_CUDA, std::string("ps_profile_steps: ") + cudaGetErrorString(le));
   s->grid_valid = true;
   return check_device_error(s);
+}
+
+extern "C" int ps_forward_checkpointed(ps_sim* s, int64_t n_steps, int64_t every) {
+  if (s == nullptr || n_steps < 1 || every < 1) return fail(PS_ERR_INVALID, "ps_forward_checkpointed: bad argument");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_forward_checkpointed: call ps_set_state first");
+  if (s->has_mesh) return fail(PS_ERR_INVALID, "ps_forward_checkpointed: differentiation supports box containers only");
+  DeviceGuard guard(s->device);
+  const int64_t n_blocks = (n_steps + every - 1) / every;
+  for (size_t k = (size_t)n_blocks + 1; k < s->fwd_ckpt.size(); ++k) cudaFree(s->fwd_ckpt[k]);
+  s->fwd_ckpt.resize((size_t)n_blocks + 1, nullptr);
+  for (int64_t blk = 0; blk < n_blocks; ++blk) {
+    int rc = save_state(s, s->fwd_ckpt[(size_t)blk]);
+    if (rc == PS_OK) rc = ps_step(s, std::min(every, n_steps - blk * every));
+    if (rc != PS_OK) return rc;
+  }
+  int rc = save_state(s, s->fwd_ckpt.back());
+  if (rc != PS_OK) return rc;
+  s->fwd_steps = n_steps;
+  s->fwd_every = every;
+  return ps_sync(s);
+}
+
+extern "C" int ps_backward(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl_dstate0) {
+  if (s == nullptr || dl_dstate == nullptr || grads == nullptr) return fail(PS_ERR_INVALID, "ps_backward: null argument");
+  if (s->fwd_steps < 1) return fail(PS_ERR_INVALID, "ps_backward: call ps_forward_checkpointed first");
+  DeviceGuard guard(s->device);
+  if (s->precision == PS_FP32)
+    return s->multi ? backward_impl<float, true>(s, dl_dstate, grads, dl_dstate0)
+                    : backward_impl<float, false>(s, dl_dstate, grads, dl_dstate0);
+  return s->multi ? backward_impl<double, true>(s, dl_dstate, grads, dl_dstate0)
+                  : backward_impl<double, false>(s, dl_dstate, grads, dl_dstate0);
 }
 
 extern "C" int ps_sync(ps_sim* s) {

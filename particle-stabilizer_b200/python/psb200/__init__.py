@@ -26,7 +26,8 @@ EXPORTED = (
     "ps_last_error", "ps_create", "ps_set_state", "ps_get_state", "ps_step", "ps_sync", "ps_stats_get",
     "ps_grid_get", "ps_buckets_get", "ps_last_launch_count", "ps_destroy", "ps_simulate",
     "ps_exclusive_scan_scratch_bytes", "ps_exclusive_scan_u32", "ps_read_csv", "ps_write_csv", "ps_read_obj",
-    "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "runSimulateCUDA",
+    "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "ps_forward_checkpointed",
+    "ps_backward", "runSimulateCUDA",
 )
 KERNEL_KINDS = ("begin", "scan", "scatter", "rank_move", "contacts")
 
@@ -47,6 +48,14 @@ class Stats(C.Structure):
 class GridInfo(C.Structure):
     _fields_ = [("min", C.c_double * 3), ("interval", C.c_double), ("nb", C.c_int32 * 3), ("n_cells", C.c_int64),
                 ("cell_base", C.c_int64), ("particle_base", C.c_int64)]
+
+
+class Grad(C.Structure):
+    _fields_ = [("k_spring", C.c_double), ("e_sphere", C.c_double), ("e_wall", C.c_double * 6)]
+
+    def as_array(self) -> np.ndarray:
+        """(k_spring, e_sphere, e_wall[0..5]) in the reference's wall order."""
+        return np.array([self.k_spring, self.e_sphere, *self.e_wall])
 
 
 class PSError(RuntimeError):
@@ -86,6 +95,8 @@ def lib() -> C.CDLL:
         L.ps_checkpoint_load.argtypes = [C.c_void_p, C.c_int32]
         L.ps_time_steps.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_double)]
         L.ps_profile_steps.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+        L.ps_forward_checkpointed.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
+        L.ps_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -200,6 +211,20 @@ class Simulation:
         _check(lib().ps_buckets_get(self.h, _ptr(counts), _ptr(offsets), _ptr(order)), "ps_buckets_get")
         return counts, offsets, order
 
+    def forward_checkpointed(self, n_steps: int, every: int) -> None:
+        """Advance n_steps keeping a checkpoint every `every` steps (for backward)."""
+        _check(lib().ps_forward_checkpointed(self.h, int(n_steps), int(every)), "ps_forward_checkpointed")
+
+    def backward(self, dl_dstate: np.ndarray):
+        """Gradients of a loss of the final state: dl_dstate is (n, 6) =
+        dL/d(x, y, z, vx, vy, vz).  Returns (per-scene (8,) arrays of
+        dL/d(k_spring, e_sphere, e_wall[6]), dL/d(initial state) (n, 6))."""
+        g = np.ascontiguousarray(dl_dstate, dtype=np.float64)
+        grads = (Grad * len(self.scenes))()
+        out = np.empty((self.n, 6), dtype=np.float64)
+        _check(lib().ps_backward(self.h, _ptr(g), grads, _ptr(out)), "ps_backward")
+        return [gr.as_array() for gr in grads], out
+
     def close(self) -> None:
         if getattr(self, "h", None):
             lib().ps_destroy(self.h)
@@ -216,6 +241,19 @@ class Simulation:
 
     def __exit__(self, *a):
         self.close()
+
+
+def height_loss(state: np.ndarray, h0: float = 0.1, amp: float = 0.02, wavelength: float = 0.5):
+    """Settling loss mean_i (z_i - h(x_i))^2, h(x) = h0 + amp sin(2 pi x / wavelength),
+    and its gradient with respect to the state (n, 6)."""
+    x, z = state[:, 0], state[:, 2]
+    w = 2.0 * np.pi / wavelength
+    r = z - (h0 + amp * np.sin(w * x))
+    n = state.shape[0]
+    g = np.zeros((n, 6))
+    g[:, 2] = 2.0 * r / n
+    g[:, 0] = -2.0 * r * amp * w * np.cos(w * x) / n
+    return float(np.mean(r * r)), g
 
 
 def simulate(scene: Scene, steps: int, precision: str = "f32") -> np.ndarray:

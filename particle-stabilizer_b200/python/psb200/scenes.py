@@ -181,6 +181,63 @@ def funnel_triangles(n_seg: int = 200, n_cone: int = 40, n_cyl: int = 6, n_ring:
     return t.astype(np.float32).astype(np.float64)
 
 
+def box_container(lo=(-0.1, -0.1, 0.0), hi=(0.1, 0.1, 0.25), n: int = 4) -> np.ndarray:
+    """Closed axis-aligned box as a triangle mesh: n x n quads per face, two
+    triangles each, normals pointing out; single-precision vertices."""
+    lo = np.asarray(lo, dtype=np.float64)
+    hi = np.asarray(hi, dtype=np.float64)
+    tris = []
+    for axis in range(3):
+        u, v = [a for a in range(3) if a != axis]
+        for side, sign in ((lo[axis], -1.0), (hi[axis], 1.0)):
+            for i in range(n):
+                for j in range(n):
+                    def pt(a, b):
+                        p = np.zeros(3)
+                        p[axis] = side
+                        p[u] = lo[u] + (hi[u] - lo[u]) * a / n
+                        p[v] = lo[v] + (hi[v] - lo[v]) * b / n
+                        return p
+                    p00, p10, p01, p11 = pt(i, j), pt(i + 1, j), pt(i, j + 1), pt(i + 1, j + 1)
+                    t1, t2 = [p00, p10, p11], [p00, p11, p01]
+                    if np.sign(np.cross(t1[1] - t1[0], t1[2] - t1[0])[axis]) != sign:
+                        t1, t2 = [p00, p11, p10], [p00, p01, p11]
+                    tris.append(np.concatenate(t1))
+                    tris.append(np.concatenate(t2))
+    return np.asarray(tris).astype(np.float32).astype(np.float64)
+
+
+def box_mesh_scene(n: int = 120, seed: int = 41) -> Scene:
+    """Spheres in a closed triangulated box; the outer layers overlap the
+    side walls and the floor from the first step.  Spring 2, dt 1e-4."""
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(5), np.arange(5), np.arange(5), indexing="ij"), -1).reshape(-1, 3)[:n]
+    pos = np.array([-0.092, -0.092, 0.006]) + g * 0.046 + rng.uniform(-0.002, 0.002, size=(n, 3))
+    vel = rng.normal(0, 0.5, size=(n, 3))
+    st = _state(pos, vel, np.full(n, 0.012), 1000.0)
+    return Scene(st, (-0.1, -0.1, 0.0), (0.1, 0.1, 0.25), (0, 0, -9.8), (0.7,) * 6, 2.0, 0.5, 1e-4,
+                 tri=box_container(), name="box_mesh")
+
+
+def funnel_wall_scene(n: int = 2000, seed: int = 7, coarse: bool = True) -> Scene:
+    """Spheres (r 0.003) on rings just inside the funnel's cone wall at
+    heights 0.45..0.9, pressing outward, plus some above the rim: every
+    step has triangle contacts.  A coarse funnel keeps the all-pairs oracle fast."""
+    rng = np.random.default_rng(seed)
+    tri = funnel_triangles(64, 12, 3, 2) if coarse else funnel_triangles()
+    z = rng.uniform(0.45, 1.05, size=n)
+    t = np.clip((1.0 - z) / 0.7, 0.0, 1.0)
+    wall_r = 0.5 + (0.08 - 0.5) * t
+    rad = wall_r - rng.uniform(0.0, 0.004, size=n)
+    th = rng.uniform(0, 2 * math.pi, size=n)
+    pos = np.stack([rad * np.cos(th), rad * np.sin(th), z], 1)
+    vel = np.stack([0.3 * np.cos(th), 0.3 * np.sin(th), rng.normal(0, 0.1, n)], 1)
+    st = _state(pos, vel, np.full(n, 0.003), 1000.0)
+    e = (0.6,) * 6
+    return Scene(st, (-0.5, -0.5, 0.0), (0.5, 0.5, 1.0), (0, 0, -9.8), e, 2e-2, 0.5, 5e-6, tri=tri, widen_domain=1,
+                 name="funnel_wall")
+
+
 def write_obj(path: str, tri: np.ndarray) -> None:
     """Triangle soup as OBJ (one vertex line per corner, %.9g = exact float)."""
     with open(path, "w") as f:

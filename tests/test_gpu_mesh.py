@@ -1,0 +1,82 @@
+"""Triangle container on the GPU (binned mesh) against the oracle's
+all-pairs restatement of PolygonContainerCUDA, bit for bit, and the CLI /
+runSimulateCUDA path with an OBJ container."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import psb200
+from psb200 import scenes
+from oracle import ps_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def run_gpu(sc, steps, precision):
+    with psb200.Simulation(sc, precision) as sim:
+        sim.set_state()
+        sim.step(steps)
+        sim.sync()
+        return sim.get_state()
+
+
+def cast(a, precision):
+    return a.astype(np.float32) if precision == "f32" else a
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("steps", [1, 7, 60])
+def test_box_mesh_bitexact(need_gpu, precision, steps):
+    sc = scenes.box_mesh_scene()
+    got = cast(run_gpu(sc, steps, precision), precision)
+    want = O.run(sc, steps, precision)
+    assert np.array_equal(got, want), f"{np.sum(np.any(got != want, axis=1))} of {sc.n} differ"
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("quirk", [1, 0])
+def test_funnel_wall_bitexact(need_gpu, precision, quirk):
+    sc = scenes.funnel_wall_scene(1500, seed=9).copy(edge_quirk=quirk)
+    got = cast(run_gpu(sc, 40, precision), precision)
+    want = O.run(sc, 40, precision)
+    # the same step with the container replaced by a loose box (no walls reached)
+    loose = sc.copy(tri=None, box_min=(-0.6, -0.6, -0.1), box_max=(0.6, 0.6, 1.2))
+    moved = np.any(O.run(loose, 1, precision) != O.run(sc, 1, precision), axis=1)
+    assert moved.sum() > 100  # the container acts on many particles every step
+    assert np.array_equal(got, want), f"{np.sum(np.any(got != want, axis=1))} of {sc.n} differ"
+
+
+def test_full_funnel_mesh_runs_with_widened_domain(need_gpu):
+    sc = scenes.funnel_wall_scene(800, seed=3, coarse=False)
+    got = run_gpu(sc, 12, "f32").astype(np.float32)
+    want = O.run(sc, 12, "f32")
+    assert np.array_equal(got, want)
+
+
+def test_cli_runs_the_path_with_an_obj_container(need_gpu, tmp_path):
+    """runSimulateCUDA through the command line: CSV in, OBJ container,
+    CSV out equal to the oracle's FP64 state written in the same format."""
+    sc = scenes.box_mesh_scene(60, seed=5)
+    obj = tmp_path / "box.obj"
+    scenes.write_obj(str(obj), sc.tri)
+    csv_in = tmp_path / "in.csv"
+    with open(csv_in, "w") as f:
+        f.write("x,y,z,r\n")
+        for p in sc.state:
+            f.write("%.17g,%.17g,%.17g,%.17g\n" % (p[0], p[1], p[2], p[6]))
+    csv_out = tmp_path / "out.csv"
+    lib = psb200.LIB_PATH
+    cmd = [psb200.CLI_PATH, "--lib", lib, str(csv_in), "--cuda", "--container", str(obj), "--max-steps", "25",
+           "--dt", "0.0001", "--coeff-of-spring", "2", "--coeff-of-restitution-sphere", "0.5",
+           "--coeff-of-restitution-wall", "0.7", "0.7", "0.7", "0.7", "0.7", "0.7", "--gravity", "0", "0", "-9.8",
+           "--initial-velocity", "0.1", "-0.2", "0.05", "--density", "1000", "--out-csv-path", str(csv_out)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Number of collided particles" in r.stdout and "nPolygons = " in r.stdout
+    start = psb200.read_csv(str(csv_in), (0.1, -0.2, 0.05), 1000.0)
+    want = O.run(sc.copy(state=start), 25, "f64")
+    ref_csv = tmp_path / "want.csv"
+    psb200.write_csv(str(ref_csv), want)
+    assert csv_out.read_text() == ref_csv.read_text()
