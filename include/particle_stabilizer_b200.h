@@ -197,6 +197,23 @@ int ps_simulate(const ps_scene_desc* scene, const double* aos_in, double* aos_ou
 size_t ps_exclusive_scan_scratch_bytes(int64_t n);
 int ps_exclusive_scan_u32(const uint32_t* d_in, uint32_t* d_out, int64_t n, void* d_scratch, void* stream);
 
+/* The same exclusive scan for callers that cannot allocate device memory:
+ * code that runs while its stream is being captured into a CUDA graph (where
+ * cudaMalloc is not allowed), real-time loops that cannot afford the device-
+ * wide synchronisation cudaMalloc/cudaFree imply, and hosts whose device
+ * memory is fully handed out to their own pool allocator.  It has no
+ * counterpart in the reference.  It allocates nothing: its scratch is a
+ * fixed array inside this library (128 KB per GPU, held from the moment the
+ * library is loaded on that GPU until the process exits), so n is limited to
+ * PS_SCAN_NOALLOC_MAX_N elements; larger n returns PS_ERR_INVALID.  The first
+ * call on each device looks up the array's device address; make that first
+ * call before any stream capture.  Every call on a device shares the one
+ * array, so calls whose kernels may overlap on the GPU (different streams
+ * without ordering) race and give wrong results: order them on one stream.
+ * d_in may equal d_out. */
+#define PS_SCAN_NOALLOC_MAX_N 134217728LL
+int ps_exclusive_scan_u32_noalloc(const uint32_t* d_in, uint32_t* d_out, int64_t n, void* stream);
+
 /* CSV particle file, the reference's format (src/ParticleStabilizer/ParticleIO.cpp:58-144):
  * header line skipped; rows x,y,z,r; mass = density*4/3*pi*r^3; velocity is
  * the given vector.  ps_read_csv returns the row count in *n_out and fills

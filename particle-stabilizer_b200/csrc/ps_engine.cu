@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1285,6 +1286,57 @@ extern "C" int ps_exclusive_scan_u32(const uint32_t* d_in, uint32_t* d_out, int6
   PS_CUDA(cudaMemsetAsync(d_scratch, 0, scan_scratch_bytes(n), st));
   k_exclusive_scan_u32<<<(unsigned)scan_num_tiles(n), SCAN_THREADS, 0, st>>>(d_in, d_out, n, static_cast<uint64_t*>(d_scratch),
                                                                              err);
+  PS_CUDA(cudaGetLastError());
+  return PS_OK;
+}
+
+// ---- exclusive scan that allocates nothing -------------------------------------
+// Scratch for ps_exclusive_scan_u32_noalloc: the ticket/error words and one
+// status word per tile, for at most PS_SCAN_NOALLOC_MAX_N elements.  Each GPU
+// holds its own copy of this array from the moment the library is loaded on
+// it until the process exits.
+namespace {
+constexpr int64_t kNoAllocMaxTiles = PS_SCAN_NOALLOC_MAX_N / SCAN_TILE;  // 16384
+constexpr int kNoAllocMaxDevices = 64;
+static_assert(PS_SCAN_NOALLOC_MAX_N % SCAN_TILE == 0, "whole tiles");
+}  // namespace
+
+static __device__ __align__(256) uint64_t g_noalloc_scan_scratch[1 + kNoAllocMaxTiles];
+
+namespace {
+// Device address of g_noalloc_scan_scratch per device, found on the first
+// call made with that device current (host code must not pass the symbol
+// itself: on the host it names a stand-in, not device memory).
+std::atomic<uint64_t*> g_noalloc_scratch_addr[kNoAllocMaxDevices];
+}  // namespace
+
+extern "C" int ps_exclusive_scan_u32_noalloc(const uint32_t* d_in, uint32_t* d_out, int64_t n, void* stream) {
+  if (n < 0 || (n > 0 && (d_in == nullptr || d_out == nullptr)))
+    return fail(PS_ERR_INVALID, "ps_exclusive_scan_u32_noalloc: bad argument");
+  if (n > PS_SCAN_NOALLOC_MAX_N)
+    return fail(PS_ERR_INVALID, "ps_exclusive_scan_u32_noalloc: n = " + std::to_string(n) +
+                                    " exceeds the fixed scratch capacity of " +
+                                    std::to_string(PS_SCAN_NOALLOC_MAX_N) + " elements");
+  if (n == 0) return PS_OK;
+  int dev = 0;
+  PS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(PS_ERR_INVALID, "ps_exclusive_scan_u32_noalloc: device id " + std::to_string(dev) + " out of range");
+  uint64_t* scratch = g_noalloc_scratch_addr[dev].load(std::memory_order_acquire);
+  if (scratch == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      return fail(PS_ERR_CUDA, std::string("ps_exclusive_scan_u32_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    scratch = static_cast<uint64_t*>(p);
+    g_noalloc_scratch_addr[dev].store(scratch, std::memory_order_release);
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // the previous call left its ticket and tile flags behind: clear what this
+  // call's tiles read
+  PS_CUDA(cudaMemsetAsync(scratch, 0, scan_scratch_bytes(n), st));
+  k_exclusive_scan_u32<<<(unsigned)scan_num_tiles(n), SCAN_THREADS, 0, st>>>(d_in, d_out, n, scratch,
+                                                                             reinterpret_cast<uint32_t*>(scratch) + 1);
   PS_CUDA(cudaGetLastError());
   return PS_OK;
 }

@@ -27,7 +27,7 @@ EXPORTED = (
     "ps_grid_get", "ps_buckets_get", "ps_last_launch_count", "ps_destroy", "ps_simulate",
     "ps_exclusive_scan_scratch_bytes", "ps_exclusive_scan_u32", "ps_read_csv", "ps_write_csv", "ps_read_obj",
     "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "ps_forward_checkpointed",
-    "ps_backward", "runSimulateCUDA",
+    "ps_backward", "ps_exclusive_scan_u32_noalloc", "runSimulateCUDA",
 )
 KERNEL_KINDS = ("begin", "scan", "scatter", "rank_move", "contacts")
 
@@ -97,6 +97,7 @@ def lib() -> C.CDLL:
         L.ps_profile_steps.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
         L.ps_forward_checkpointed.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
         L.ps_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ps_exclusive_scan_u32_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
         _lib = L
     return _lib
 
@@ -270,6 +271,16 @@ def exclusive_scan_u32(d_in: int, d_out: int, n: int, d_scratch: int, stream: in
     """ps_exclusive_scan_u32 on device pointers (integers)."""
     _check(lib().ps_exclusive_scan_u32(C.c_void_p(d_in), C.c_void_p(d_out), int(n), C.c_void_p(d_scratch),
                                        C.c_void_p(stream)), "ps_exclusive_scan_u32")
+
+
+SCAN_NOALLOC_MAX_N = 134217728
+
+
+def exclusive_scan_u32_noalloc(d_in: int, d_out: int, n: int, stream: int = 0) -> None:
+    """ps_exclusive_scan_u32_noalloc on device pointers: the scan without any
+    allocation, using the library's fixed scratch array (n <= SCAN_NOALLOC_MAX_N)."""
+    _check(lib().ps_exclusive_scan_u32_noalloc(C.c_void_p(d_in), C.c_void_p(d_out), int(n), C.c_void_p(stream)),
+           "ps_exclusive_scan_u32_noalloc")
 
 
 def exclusive_scan_scratch_bytes(n: int) -> int:
