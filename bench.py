@@ -202,6 +202,124 @@ def reference_cpu_sample(scene, budget_s: float, max_steps: int, warmup: int = 0
             "seconds": t, "steps": steps}
 
 
+def non_finite(state) -> int:
+    """Particles with a non-finite coordinate: the reference scheme's kick
+    k*overlap/m is not scaled by dt and diverges once k*dt/m is well above 1."""
+    return int(np.sum(~np.isfinite(state[:, :6]).all(axis=1)))
+
+
+def adjoint_measure(psb200, sc, steps, every, device, restore_block=None) -> dict:
+    """Plain forward vs checkpointed forward + backward on one scene (FP32),
+    device/wall time with a synchronize on both sides."""
+    with psb200.Simulation(sc, "f32", device=device) as sim:
+        sim.set_state()
+        sim.checkpoint_save(0)
+        sim.time_steps(min(steps, 20))  # warm-up: graphs captured
+        sim.checkpoint_load(0)
+        fwd_ms = sim.time_steps(steps)
+        sim.checkpoint_load(0)
+        sim.forward_checkpointed(steps, every)  # warm-up of the backward path
+        _, g = psb200.height_loss(sim.get_state())
+        sim.backward(g)
+        sim.checkpoint_load(0)
+        sim.sync()
+        t0 = time.perf_counter()
+        sim.forward_checkpointed(steps, every)
+        t1 = time.perf_counter()
+        final = sim.get_state()
+        loss, g = psb200.height_loss(final)
+        t2 = time.perf_counter()
+        grads, _ = sim.backward(g)
+        t3 = time.perf_counter()
+    fwd_adj_s = (t1 - t0) + (t3 - t2)
+    bad = non_finite(final)
+    return {"scene": sc.name, "n_particles": sc.n, "steps": steps, "checkpoint_every": every,
+            "forward_ms": fwd_ms, "forward_particle_steps_per_s": sc.n * steps / (fwd_ms * 1e-3),
+            "forward_plus_adjoint_ms": 1e3 * fwd_adj_s,
+            "forward_plus_adjoint_particle_steps_per_s": sc.n * steps / fwd_adj_s,
+            "ratio_fwd_adj_over_fwd": fwd_adj_s / (fwd_ms * 1e-3), "loss": loss, "non_finite_at_end": bad,
+            "grad_k_spring": float(grads[0][0]), "grad_e_sphere": float(grads[0][1]),
+            "grad_e_wall_zmin_zmax_xmin_xmax_ymin_ymax": [float(x) for x in grads[0][2:8]],
+            "k_spring": sc.k_spring}
+
+
+def batch_measure(psb200, scenes_mod, device, steps: int, n_scenes: int, sequential: bool = True,
+                  k_range=(5e3, 5e4)) -> dict:
+    """256 uneven independent scenes: one simulation advancing all of them per
+    launch, against the same scenes run one after another, each as its own
+    simulation (steps from each scene's initial state, FP32)."""
+    batch = scenes_mod.c5_scenes(n_scenes, k_range=k_range)
+    n_total = sum(s.n for s in batch)
+    with psb200.Simulation(batch, "f32", device=device) as sim:
+        sim.set_state()
+        sim.checkpoint_save(0)
+        sim.time_steps(steps)
+        sim.checkpoint_load(0)
+        batched_ms = sim.time_steps(steps)
+        launches = sim.launches()
+        bad = non_finite(sim.get_state())
+    out = {"n_scenes": n_scenes, "n_particles": n_total, "k_range": list(k_range), "steps": steps,
+           "batched_ms": batched_ms,
+           "batched_scene_steps_per_s": n_scenes * steps / (batched_ms * 1e-3),
+           "batched_particle_steps_per_s": n_total * steps / (batched_ms * 1e-3),
+           "launches_batched": launches, "non_finite_at_end": bad}
+    if not sequential:
+        return out
+    seq_ms = 0.0
+    seq_launches = 0
+    for sc in batch:
+        with psb200.Simulation(sc, "f32", device=device) as s1:
+            s1.set_state()
+            s1.checkpoint_save(0)
+            s1.time_steps(steps)
+            s1.checkpoint_load(0)
+            seq_ms += s1.time_steps(steps)
+            seq_launches += s1.launches()
+    out.update({"sequential_ms": seq_ms, "sequential_scene_steps_per_s": n_scenes * steps / (seq_ms * 1e-3),
+                "speedup_batched_over_sequential": seq_ms / batched_ms, "launches_sequential": seq_launches})
+    return out
+
+
+def mesh_measure(psb200, scenes_mod, device, steps: int) -> dict:
+    """262,144 spheres poured into the 20,200-triangle funnel (grid domain
+    widened over the spawn lattice), FP32, `steps` steps from the initial
+    state in one timed call."""
+    sc = scenes_mod.c3_scene()
+    with psb200.Simulation(sc, "f32", device=device) as sim:
+        sim.set_state()
+        sim.checkpoint_save(0)
+        sim.time_steps(200)
+        sim.checkpoint_load(0)
+        ms = sim.time_steps(steps)
+        st = sim.get_state()
+        launches = sim.launches()
+    below_rim = int(np.sum(st[:, 2] < 1.0))
+    return {"scene": sc.name, "n_particles": sc.n, "n_triangles": int(sc.tri.shape[0]), "steps": steps,
+            "ms": ms, "particle_steps_per_s": sc.n * steps / (ms * 1e-3), "launches": launches,
+            "particles_below_rim_at_end": below_rim, "non_finite_at_end": non_finite(st)}
+
+
+# Secondary measurements.  The reference's contact kick k*overlap/m is not
+# scaled by dt, so the scheme is stable only for k*dt/m below about 1.  The
+# differentiation and batch scenes with their specified springs (k*dt/m = 373
+# and 27..7,460) diverge at their first contacts, so each is measured twice:
+# as specified over a window before or through its divergence (the line
+# reports how many particles went non-finite), and with soft springs that keep
+# every particle finite (differentiation scene k = 5; batch springs
+# log-uniform in [0.25, 2.5]; all other draws identical).
+EXTRAS = {
+    # forward vs forward + adjoint, checkpoint every 100 steps
+    "adjoint": lambda p, s, dev, a: adjoint_measure(p, s.c4_scene(k_spring=5.0), 2000, 100, dev),
+    "adjoint_as_specified": lambda p, s, dev, a: adjoint_measure(p, s.c4_scene(), 1000, 100, dev),
+    "adjoint_1m": lambda p, s, dev, a: adjoint_measure(p, s.c4_scene(1 << 20, edge=0.95, k_spring=5.0), 2000, 100,
+                                                       dev),
+    "batch": lambda p, s, dev, a: batch_measure(p, s, dev, 100, 256, sequential=not a.no_sequential,
+                                                k_range=(0.25, 2.5)),
+    "batch_as_specified": lambda p, s, dev, a: batch_measure(p, s, dev, 100, 256, sequential=not a.no_sequential),
+    "mesh": lambda p, s, dev, a: mesh_measure(p, s, dev, 20000),
+}
+
+
 def run_ours(args, world, rank, local, dist):
     import psb200
     from psb200 import scenes
@@ -287,9 +405,12 @@ def run_ours(args, world, rank, local, dist):
         "clocks": clk.summary(),
         "wall_s": wall,
     }
+    sim.close()
+    if not args.no_extras:
+        for name in EXTRAS:
+            line[name] = EXTRAS[name](psb200, scenes, local, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = reference_cpu_sample(sc, args.cpu_budget, 20)
-    sim.close()
     return line
 
 
@@ -321,7 +442,19 @@ def main():
     ap.add_argument("--block", type=int, default=100, help="steps per block; the state is restored between blocks")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference CPU stepping")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the adjoint, batch and mesh measurements")
+    ap.add_argument("--extra", choices=sorted(EXTRAS),
+                    help="run only this secondary measurement on the local GPU and print its JSON")
+    ap.add_argument("--no-sequential", action="store_true",
+                    help="with --extra batch: skip the scene-by-scene comparison")
     args = ap.parse_args()
+    if args.extra is not None:
+        import psb200
+        from psb200 import scenes
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        print(json.dumps({args.extra: EXTRAS[args.extra](psb200, scenes, local, args)}), flush=True)
+        return
     if args.impl == "reference":
         # rank 0 alone times the reference's CPU simulator; other ranks exit
         world = int(os.environ.get("WORLD_SIZE", "1"))

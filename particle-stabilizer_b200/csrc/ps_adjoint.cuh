@@ -10,8 +10,10 @@
 // Reverse sweep of one step, given the adjoints (xbar, vbar) of its output:
 //   k_adj_contacts   (sorted order, gather): for each particle, the terms of
 //                    the pairs where it receives and the pairs where it is the
-//                    source (pairs are symmetric), so no atomics; per-particle
-//                    partials of dL/dk and dL/de_sphere.
+//                    source (pairs are symmetric), so no atomics; partials of
+//                    dL/dk and dL/de_sphere accumulated per sorted slot (a
+//                    scene owns a fixed slot range, so per-scene sums are
+//                    unchanged and the order is fixed by the canonical sort).
 //   k_adj_walls_integrate (original order): through the walls (clamp events
 //                    recomputed from the recorded step input) and the
 //                    integrate; per-particle partials of dL/de_wall.
@@ -23,17 +25,19 @@
 
 namespace psb {
 
-enum : int { ADJ_K = 0, ADJ_E = 1, ADJ_WALL = 2 };  // acc layout: k, e_sphere, e_wall[6] (zMin..yMax)
+enum : int { ADJ_K = 0, ADJ_E = 1, ADJ_WALL = 2 };  // acc rows: k, e_sphere, e_wall[6] (zMin..yMax)
 constexpr int ADJ_NACC = 8;
 
 template <class T>
 struct AdjBufs {
   const vec4_t<T>* tape;  // step input, original order: [2*o] = (x, r), [2*o+1] = (v, m)
-  T* ax;                  // adjoint of positions (3 per particle, original order)
-  T* av;                  // adjoint of velocities
-  T* ax2;                 // output of k_adj_contacts
-  T* av2;
-  double* acc;            // ADJ_NACC per particle, original order, accumulated over steps
+  vec4_t<T>* ax;          // adjoint of positions, original order (w unused): one 16/32-B access
+  vec4_t<T>* av;          // adjoint of velocities
+  vec4_t<T>* ax2;         // output of k_adj_contacts
+  vec4_t<T>* av2;
+  double* acc;            // ADJ_NACC rows of n, accumulated over steps: rows k, e by sorted
+                          // slot, wall rows by original index
+  uint32_t n;             // row length of acc
 };
 
 // Terms of one active pair for the receiver r and the source s:
@@ -83,8 +87,9 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, Ad
   const vec4_t<T> P = b.P0[i];
   const vec4_t<T> V = b.V0[i];
   const uint32_t oi = b.orig[i];
-  const T gx = a.av[3 * oi], gy = a.av[3 * oi + 1], gz = a.av[3 * oi + 2];
-  T xb0 = a.ax[3 * oi], xb1 = a.ax[3 * oi + 1], xb2 = a.ax[3 * oi + 2];
+  const vec4_t<T> G = a.av[oi], X = a.ax[oi];
+  const T gx = G.x, gy = G.y, gz = G.z;
+  T xb0 = X.x, xb1 = X.y, xb2 = X.z;
   T vb0 = gx, vb1 = gy, vb2 = gz;
   double dk = 0.0, de = 0.0;
   int32_t cx, cy, cz;
@@ -93,9 +98,10 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, Ad
   const uint32_t z0 = (uint32_t)(cz > 0 ? cz - 1 : 0);
   const uint32_t z1 = (uint32_t)(cz + 1 < nz ? cz + 1 : nz - 1) + 1u;
   const T k = sp.k_spring, e = sp.e_sphere;
+  const bool live = isfinite(P.x) && isfinite(P.y) && isfinite(P.z);  // no active pair otherwise
   for (int q = 0; q < 9; ++q) {
     const int32_t bx = cx - 1 + q / 3, by = cy - 1 + q % 3;
-    if (bx < 0 || bx >= nx || by < 0 || by >= ny) continue;
+    if (!live || bx < 0 || bx >= nx || by < 0 || by >= ny) continue;
     const uint32_t col = sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz;
     const uint32_t j0 = b.offset[col + z0], j1 = b.offset[col + z1];
     for (uint32_t j = j0; j < j1; ++j) {
@@ -118,7 +124,8 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, Ad
       vb2 += duz;
       // j receives from i: i enters as the source (d and u change sign)
       double dk2 = 0.0, de2 = 0.0;
-      const T hx = a.av[3 * oj], hy = a.av[3 * oj + 1], hz = a.av[3 * oj + 2];
+      const vec4_t<T> H = a.av[oj];
+      const T hx = H.x, hy = H.y, hz = H.z;
       pair_adjoint<T>(-dx, -dy, -dz, -ux, -uy, -uz, R, Vj.w, V.w, k, e, hx, hy, hz, ddx, ddy, ddz, dux, duy, duz, dk2,
                       de2);
       xb0 -= ddx;
@@ -129,14 +136,17 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, Ad
       vb2 -= duz;
     }
   }
-  a.ax2[3 * oi] = xb0;
-  a.ax2[3 * oi + 1] = xb1;
-  a.ax2[3 * oi + 2] = xb2;
-  a.av2[3 * oi] = vb0;
-  a.av2[3 * oi + 1] = vb1;
-  a.av2[3 * oi + 2] = vb2;
-  a.acc[ADJ_NACC * oi + ADJ_K] += dk;
-  a.acc[ADJ_NACC * oi + ADJ_E] += de;
+  vec4_t<T> xo = X, vo = G;
+  xo.x = xb0;
+  xo.y = xb1;
+  xo.z = xb2;
+  vo.x = vb0;
+  vo.y = vb1;
+  vo.z = vb2;
+  a.ax2[oi] = xo;
+  a.av2[oi] = vo;
+  a.acc[(size_t)ADJ_K * a.n + i] += dk;
+  a.acc[(size_t)ADJ_E * a.n + i] += de;
 }
 
 // Walls + integrate adjoint, original order.  The step input (x, v) comes
@@ -155,26 +165,39 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_walls_integrate(StepBufs<T
   const T r = P.w;
   const T xs[3] = {P.x, P.y, P.z}, vs[3] = {V.x, V.y, V.z};
   const int lo_idx[3] = {PS_XMIN, PS_YMIN, PS_ZMIN}, hi_idx[3] = {PS_XMAX, PS_YMAX, PS_ZMAX};
-  double* acc = a.acc + ADJ_NACC * (size_t)o;
+  double* acc = a.acc + o;  // row c at acc[c * n]
+  const vec4_t<T> X2 = a.ax2[o], V2 = a.av2[o];
+  const T xb2[3] = {X2.x, X2.y, X2.z}, vb2[3] = {V2.x, V2.y, V2.z};
+  T xo[3], vo[3];
+#pragma unroll
   for (int ax = 0; ax < 3; ++ax) {
     const bool lo_hit = A::sub(xs[ax], r) < sp.box_lo[ax];
     const bool hi_hit = A::add(xs[ax], r) > sp.box_hi[ax];
-    T xb = a.ax2[3 * o + ax], vb = a.av2[3 * o + ax];
+    T xb = xb2[ax], vb = vb2[ax];
     const T v1 = lo_hit ? A::mul(-vs[ax], sp.e_lo[ax]) : vs[ax];  // velocity after the min clamp
     if (hi_hit) {
-      acc[ADJ_WALL + hi_idx[ax]] += (double)(-v1 * vb);
+      acc[(size_t)(ADJ_WALL + hi_idx[ax]) * a.n] += (double)(-v1 * vb);
       vb = -sp.e_hi[ax] * vb;
       xb = T(0);
     }
     if (lo_hit) {
-      acc[ADJ_WALL + lo_idx[ax]] += (double)(-vs[ax] * vb);
+      acc[(size_t)(ADJ_WALL + lo_idx[ax]) * a.n] += (double)(-vs[ax] * vb);
       vb = -sp.e_lo[ax] * vb;
       xb = T(0);
     }
     // integrate: x' = x + v dt, v' = v + g dt
-    a.ax[3 * o + ax] = xb;
-    a.av[3 * o + ax] = vb + sp.dt * xb;
+    xo[ax] = xb;
+    vo[ax] = vb + sp.dt * xb;
   }
+  vec4_t<T> xw = X2, vw = V2;
+  xw.x = xo[0];
+  xw.y = xo[1];
+  xw.z = xo[2];
+  vw.x = vo[0];
+  vw.y = vo[1];
+  vw.z = vo[2];
+  a.ax[o] = xw;
+  a.av[o] = vw;
 }
 
 // Gather the at-rest state (P0, V1) into the tape row in original order.
@@ -197,7 +220,8 @@ __global__ void k_tape_read(StepBufs<T> b, const vec4_t<T>* row) {
   b.orig[o] = o;
 }
 
-// Per-scene sums of the per-particle parameter partials, in a fixed order.
+// Per-scene sums of the parameter partials (acc: ADJ_NACC rows of n), in a
+// fixed order.
 __global__ void k_adj_reduce(const double* acc, const uint32_t* pbase, int n_scenes, uint32_t n, double* out) {
   const int s = blockIdx.x;
   if (s >= n_scenes) return;
@@ -206,7 +230,7 @@ __global__ void k_adj_reduce(const double* acc, const uint32_t* pbase, int n_sce
   double loc[ADJ_NACC];
   for (int c = 0; c < ADJ_NACC; ++c) loc[c] = 0.0;
   for (uint32_t p = p0 + threadIdx.x; p < p1; p += blockDim.x)
-    for (int c = 0; c < ADJ_NACC; ++c) loc[c] += acc[ADJ_NACC * (size_t)p + c];
+    for (int c = 0; c < ADJ_NACC; ++c) loc[c] += acc[(size_t)c * n + p];
   for (int c = 0; c < ADJ_NACC; ++c) red[c][threadIdx.x] = loc[c];
   __syncthreads();
   for (int w = 64; w > 0; w >>= 1) {

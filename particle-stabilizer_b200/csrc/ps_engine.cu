@@ -798,30 +798,32 @@ void enqueue_prepare(ps_sim* s) {
 }
 
 template <class T>
-__global__ void k_adj_upload(const double* __restrict__ g, T* ax, T* av, uint32_t n) {
+__global__ void k_adj_upload(const double* __restrict__ g, vec4_t<T>* ax, vec4_t<T>* av, uint32_t n) {
   const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= n) return;
-  for (int c = 0; c < 3; ++c) {
-    ax[3 * o + c] = (T)g[6 * (size_t)o + c];
-    av[3 * o + c] = (T)g[6 * (size_t)o + 3 + c];
-  }
+  const double* q = g + 6 * (size_t)o;
+  vec4_t<T> x, v;
+  x.x = (T)q[0]; x.y = (T)q[1]; x.z = (T)q[2]; x.w = T(0);
+  v.x = (T)q[3]; v.y = (T)q[4]; v.z = (T)q[5]; v.w = T(0);
+  ax[o] = x;
+  av[o] = v;
 }
 
 template <class T>
-__global__ void k_adj_download(const T* ax, const T* av, double* __restrict__ g, uint32_t n) {
+__global__ void k_adj_download(const vec4_t<T>* ax, const vec4_t<T>* av, double* __restrict__ g, uint32_t n) {
   const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= n) return;
-  for (int c = 0; c < 3; ++c) {
-    g[6 * (size_t)o + c] = (double)ax[3 * o + c];
-    g[6 * (size_t)o + 3 + c] = (double)av[3 * o + c];
-  }
+  const vec4_t<T> x = ax[o], v = av[o];
+  double* q = g + 6 * (size_t)o;
+  q[0] = (double)x.x; q[1] = (double)x.y; q[2] = (double)x.z;
+  q[3] = (double)v.x; q[4] = (double)v.y; q[5] = (double)v.z;
 }
 
 template <class T, bool MULTI>
 int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl_dstate0) {
   const int64_t n = s->n_total, K = s->fwd_every;
   const size_t tape_b = align_up(2 * sizeof(vec4_t<T>) * (size_t)n * (size_t)K, 256);
-  const size_t adj_b = align_up(3 * sizeof(T) * (size_t)n, 256);
+  const size_t adj_b = align_up(sizeof(vec4_t<T>) * (size_t)n, 256);
   const size_t acc_b = align_up(ADJ_NACC * sizeof(double) * (size_t)n, 256);
   const size_t io_b = align_up(6 * sizeof(double) * (size_t)n, 256);
   const size_t red_b = align_up(ADJ_NACC * sizeof(double) * (size_t)s->n_scenes, 256);
@@ -838,11 +840,12 @@ int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl
   p += tape_b;
   AdjBufs<T> a;
   a.tape = tape;
-  a.ax = reinterpret_cast<T*>(p); p += adj_b;
-  a.av = reinterpret_cast<T*>(p); p += adj_b;
-  a.ax2 = reinterpret_cast<T*>(p); p += adj_b;
-  a.av2 = reinterpret_cast<T*>(p); p += adj_b;
+  a.ax = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
+  a.av = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
+  a.ax2 = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
+  a.av2 = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
   a.acc = reinterpret_cast<double*>(p); p += acc_b;
+  a.n = (uint32_t)n;
   double* io = reinterpret_cast<double*>(p); p += io_b;
   double* red = reinterpret_cast<double*>(p);
   cudaStream_t st = s->stream;

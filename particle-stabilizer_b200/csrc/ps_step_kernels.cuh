@@ -338,11 +338,16 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 5 : 4) k_contac
     const int32_t nx = sp.nb[0], ny = sp.nb[1], nz = sp.nb[2];
     const uint32_t z0 = (uint32_t)(cz > 0 ? cz - 1 : 0);
     const uint32_t z1 = (uint32_t)(cz + 1 < nz ? cz + 1 : nz - 1) + 1u;
+    // A particle whose own position is not finite has no contact: every
+    // pair gives d2 = inf (rejected by the filter) or NaN (overlap NaN), so
+    // its candidate loop is skipped.  Diverged particles all hash to a few
+    // cells, where the loop would otherwise be quadratic.
+    const bool live = isfinite(P.x) && isfinite(P.y) && isfinite(P.z);
     uint32_t lo[9], hi[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
       const int32_t bx = cx - 1 + q / 3, by = cy - 1 + q % 3;
-      const bool ok = bx >= 0 && bx < nx && by >= 0 && by < ny;
+      const bool ok = live && bx >= 0 && bx < nx && by >= 0 && by < ny;
       // in-range address even where the column does not exist
       const uint32_t col = ok ? sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz : sp.cbase;
       lo[q] = ok ? __ldg(b.offset + col + z0) : 0u;

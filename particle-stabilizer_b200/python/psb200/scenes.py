@@ -116,6 +116,40 @@ def pile(n: int = 1024, seed: int = 3, k_spring: float = 1.0, e_sphere: float = 
                  name="pile")
 
 
+def settle_pile(side: int = 16, seed: int = 9) -> Scene:
+    """Long-run fixture: side^3 spheres of radius 0.01 at rest on a lattice of
+    pitch 0.0225 (jitter +-0.001) in a box of base (side * 0.0225)^2 and
+    height 1, spring 40 (k dt / m = 0.095, stable under the reference
+    scheme), sphere restitution 0.5, walls 0.5, dt 1e-5.  The lattice
+    collapses into a pile that is close to rest after about 40,000 steps."""
+    rng = np.random.default_rng(seed)
+    pitch, r = 0.0225, 0.01
+    ijk = np.stack(np.meshgrid(np.arange(side), np.arange(side), np.arange(side), indexing="ij"), -1)
+    ijk = ijk.reshape(-1, 3).astype(np.float64)
+    pos = (ijk + 0.5) * pitch + rng.uniform(-0.001, 0.001, size=ijk.shape)
+    st = _state(pos, np.zeros_like(pos), np.full(pos.shape[0], r), 1000.0)
+    edge = side * pitch
+    return Scene(st, (0, 0, 0), (edge, edge, 1.0), (0, 0, -9.8), (0.5,) * 6, 40.0, 0.5, 1e-5, name="settle_pile")
+
+
+def slab_packing_fraction(state: np.ndarray, box_min, box_max, z_lo: float, z_hi: float) -> float:
+    """Fraction of the box's volume between the planes z_lo and z_hi that the
+    spheres fill (exact sphere-slab intersection volumes; the spheres are
+    inside the box and overlaps are small)."""
+    z, r = state[:, 2], state[:, 6]
+    t1 = np.clip(z_lo - z, -r, r)
+    t2 = np.clip(z_hi - z, -r, r)
+    vol = np.pi * ((r * r * t2 - t2 ** 3 / 3.0) - (r * r * t1 - t1 ** 3 / 3.0))
+    area = (box_max[0] - box_min[0]) * (box_max[1] - box_min[1])
+    return float(vol.sum() / (area * (z_hi - z_lo)))
+
+
+def height_histogram(state: np.ndarray, z_max: float, bins: int = 24) -> np.ndarray:
+    """Fraction of sphere centres in each of `bins` equal height bins over [0, z_max]."""
+    h, _ = np.histogram(state[:, 2], bins=bins, range=(0.0, z_max))
+    return h / max(1, state.shape[0])
+
+
 # ---- the 1M-sphere workload ---------------------------------------------------
 def c2_scene(n: int = 1 << 20, seed: int = 2) -> Scene:
     """1,048,576 spheres, log-normal radii (median 0.002, sigma 0.25, clipped to
@@ -270,28 +304,46 @@ def c3_scene(n: int = 262144, seed: int = 4, widen: bool = True) -> Scene:
 
 
 # ---- differentiation workload -----------------------------------------------
-def c4_scene(n: int = 65536, seed: int = 5) -> Scene:
+def c4_scene(n: int = 65536, seed: int = 5, edge: float = 0.5, k_spring: float = 1e4) -> Scene:
     """65,536 spheres of radius 0.004 in the box [0,0.5]^3 placed without
     overlap on a grid of 0.009 slots, velocities N(0, 0.01^2), spring 1e4,
-    sphere restitution 0.5, walls 0.8, dt 1e-5.  Density 1000."""
+    sphere restitution 0.5, walls 0.8, dt 1e-5.  Density 1000.  `edge`
+    enlarges the box for larger n (1M spheres need edge >= 0.918).
+
+    The reference's contact kick k*overlap/m is not scaled by dt, so the
+    explicit update is stable only for k*dt/m below about 1; with spring 1e4
+    that ratio is 373 and the first sphere-sphere contacts (after about
+    1,300 steps, when the lowest layers meet) diverge.  k_spring=5 (ratio
+    0.19) keeps the scene finite with contacts."""
     rng = np.random.default_rng(seed)
     slot = 0.009
-    d = int(0.5 / slot)
+    d = int(edge / slot)
+    if n > d ** 3:
+        raise ValueError(f"{n} spheres do not fit {d}^3 slots")
     chosen = rng.choice(d ** 3, size=n, replace=False)
     ijk = np.stack([chosen // (d * d), (chosen // d) % d, chosen % d], axis=1).astype(np.float64)
     pos = (ijk + 0.5) * slot + rng.uniform(-2e-4, 2e-4, size=(n, 3))
     vel = rng.normal(0.0, 0.01, size=(n, 3))
     st = _state(pos, vel, np.full(n, 0.004), 1000.0)
-    return Scene(st, (0, 0, 0), (0.5, 0.5, 0.5), (0, 0, -9.8), (0.8,) * 6, 1e4, 0.5, 1e-5, name="c4_65k")
+    name = "c4_65k" if (n, edge) == (65536, 0.5) else f"c4_{n}_edge{edge:g}"
+    if k_spring != 1e4:
+        name += f"_k{k_spring:g}"
+    return Scene(st, (0, 0, 0), (edge, edge, edge), (0, 0, -9.8), (0.8,) * 6, k_spring, 0.5, 1e-5, name=name)
 
 
 # ---- batching workload ---------------------------------------------------------
-def c5_scenes(n_scenes: int = 256, seed: int = 6, n_lo: int = 1024, n_hi: int = 65536) -> list[Scene]:
+def c5_scenes(n_scenes: int = 256, seed: int = 6, n_lo: int = 1024, n_hi: int = 65536,
+              k_range: tuple[float, float] = (5e3, 5e4)) -> list[Scene]:
     """Independent scenes: particle count log-uniform in [n_lo, n_hi], radii
     uniform in [0.002, 0.006], cubic box of edge uniform in [0.2, 1.0],
-    spring log-uniform in [5e3, 5e4], restitutions uniform in [0.3, 0.9],
-    dt 5e-6.  Spheres are placed without overlap on 2*r_max slots (the count
-    is capped by the slots the box holds)."""
+    spring log-uniform in k_range (default [5e3, 5e4]), restitutions uniform
+    in [0.3, 0.9], dt 5e-6.  Spheres are placed without overlap on 2*r_max
+    slots (the count is capped by the slots the box holds).
+
+    With the default springs k*dt/m reaches 27..7,460 and the reference's
+    scheme diverges at the first contacts; k_range=(0.25, 2.5) keeps
+    k*dt/m <= 0.37 and every scene finite.  The other draws do not depend on
+    k_range, so both sets share particle counts, radii, boxes and states."""
     rng = np.random.default_rng(seed)
     out = []
     for s in range(n_scenes):
@@ -306,7 +358,8 @@ def c5_scenes(n_scenes: int = 256, seed: int = 6, n_lo: int = 1024, n_hi: int = 
         ijk = np.stack([chosen // (d * d), (chosen // d) % d, chosen % d], axis=1).astype(np.float64)
         pos = (ijk + 0.5) * slot + rng.uniform(-1, 1, size=(n, 3)) * (slot / 2 - r)[:, None]
         vel = rng.normal(0.0, 0.05, size=(n, 3))
-        k = float(math.exp(rng.uniform(math.log(5e3), math.log(5e4))))
+        u = rng.uniform(0.0, 1.0)
+        k = float(math.exp(math.log(k_range[0]) + u * (math.log(k_range[1]) - math.log(k_range[0]))))
         e_s = float(rng.uniform(0.3, 0.9))
         e_w = tuple(float(x) for x in rng.uniform(0.3, 0.9, size=6))
         out.append(Scene(_state(pos, vel, r, 1000.0), (0, 0, 0), (edge, edge, edge), (0, 0, -9.8), e_w, k, e_s, 5e-6,

@@ -1,0 +1,78 @@
+"""Long runs: the 4,096-sphere settling pile (psb200.scenes.settle_pile)
+over 40,000 steps, from a lattice at rest to a pile close to rest.
+
+- FP64 on the GPU equals the oracle's FP64 run bit for bit: the SHA-256 of
+  the final state matches the committed fixture made by
+  tests/golden/make_golden_settle.py.
+- FP32 on the GPU, and the reference's own CUDA build (FP64, atomics in
+  arbitrary order), follow different trajectories after a few thousand
+  steps (the dynamics are chaotic), so they are compared by the settled
+  pile's statistics: the packing fraction of the slab z in [0.02, 0.16],
+  the height histogram of the sphere centres and the mean centre height,
+  each within the tolerance written below.
+"""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+import psb200
+from psb200 import scenes
+from oracle import ps_oracle as O
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+G = np.load(os.path.join(GOLDEN, "settle_pile_f64.npz"))
+STEPS = int(G["steps"])
+SLAB = tuple(float(x) for x in G["slab"])
+HIST_TOP = float(G["hist_top"])
+
+# Tolerances for runs that are not bit-identical to the oracle's FP64 run.
+PACKING_TOL = 0.01   # absolute, on a packing fraction of about 0.5
+HIST_TV_TOL = 0.06   # total-variation distance between height histograms
+ZMEAN_TOL = 0.01     # relative, on the mean centre height
+
+
+def summary(sc, state):
+    return (scenes.slab_packing_fraction(state, sc.box_min, sc.box_max, *SLAB),
+            scenes.height_histogram(state, HIST_TOP, len(G["hist"])),
+            float(np.mean(state[:, 2])))
+
+
+def check_statistics(sc, state):
+    packing, hist, zmean = summary(sc, state)
+    assert np.isfinite(state).all()
+    assert abs(packing - float(G["packing"])) <= PACKING_TOL, (packing, float(G["packing"]))
+    tv = 0.5 * float(np.abs(hist - G["hist"]).sum())
+    assert tv <= HIST_TV_TOL, tv
+    assert abs(zmean - float(G["zmean"])) <= ZMEAN_TOL * float(G["zmean"]), (zmean, float(G["zmean"]))
+
+
+def gpu_run(precision):
+    sc = scenes.settle_pile()
+    with psb200.Simulation(sc, precision) as sim:
+        sim.set_state()
+        sim.step(STEPS)
+        return sc, sim.get_state()
+
+
+def test_fp64_long_run_bitexact(need_gpu):
+    sc, st = gpu_run("f64")
+    assert hashlib.sha256(np.ascontiguousarray(st).tobytes()).hexdigest() == str(G["sha256"])
+    check_statistics(sc, st)
+
+
+def test_fp32_long_run_statistics(need_gpu):
+    sc, st = gpu_run("f32")
+    check_statistics(sc, st)
+
+
+@pytest.mark.skipif(not os.path.exists(O.REF_CUDA_SO),
+                    reason="oracle/_ref/libref_cuda.so was not built (reference sources absent)")
+def test_reference_cuda_long_run_statistics(need_gpu):
+    sc = scenes.settle_pile()
+    st = O.run_reference("cuda", sc, STEPS)
+    check_statistics(sc, st)
