@@ -14,9 +14,13 @@
 //                    dL/dk and dL/de_sphere accumulated per sorted slot (a
 //                    scene owns a fixed slot range, so per-scene sums are
 //                    unchanged and the order is fixed by the canonical sort).
-//   k_adj_walls_integrate (original order): through the walls (clamp events
-//                    recomputed from the recorded step input) and the
-//                    integrate; per-particle partials of dL/de_wall.
+//   k_adj_walls_integrate (the tape row's sorted order): through the walls
+//                    (clamp events recomputed from the recorded step input)
+//                    and the integrate; partials of dL/de_wall by slot.
+// The tape holds each step's input as the at-rest state in sorted order
+// (positions, velocities, original ids): rows are written and read with
+// coalesced accesses, and replaying a step starts from a spatially sorted
+// state, so its hash-and-count pass aggregates its atomics.
 // Wall clamps and contact activation are piecewise events taken from the
 // forward values; radii and masses are constants.
 #pragma once
@@ -29,8 +33,15 @@ enum : int { ADJ_K = 0, ADJ_E = 1, ADJ_WALL = 2 };  // acc rows: k, e_sphere, e_
 constexpr int ADJ_NACC = 8;
 
 template <class T>
+struct TapeRow {
+  vec4_t<T>* p;  // (x, r) per sorted slot
+  vec4_t<T>* v;  // (v, m)
+  uint32_t* o;   // original id
+};
+
+template <class T>
 struct AdjBufs {
-  const vec4_t<T>* tape;  // step input, original order: [2*o] = (x, r), [2*o+1] = (v, m)
+  TapeRow<T> tape;        // input of the step being reversed
   vec4_t<T>* ax;          // adjoint of positions, original order (w unused): one 16/32-B access
   vec4_t<T>* av;          // adjoint of velocities
   vec4_t<T>* ax2;         // output of k_adj_contacts
@@ -149,23 +160,24 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, Ad
   a.acc[(size_t)ADJ_E * a.n + i] += de;
 }
 
-// Walls + integrate adjoint, original order.  The step input (x, v) comes
-// from the tape; x' and v' and the clamp events are recomputed from it with
-// the forward's operations.
+// Walls + integrate adjoint over the tape row's sorted slots.  The step
+// input (x, v) comes from the tape; x' and v' and the clamp events are
+// recomputed from it with the forward's operations.
 template <class T, bool MULTI>
 __global__ void __launch_bounds__(STEP_THREADS) k_adj_walls_integrate(StepBufs<T> b, AdjBufs<T> a,
                                                                       SceneParams<T> sp0) {
-  const uint32_t o = blockIdx.x * STEP_THREADS + threadIdx.x;
-  if (o >= b.n) return;
-  const SceneParams<T>& sp = scene_of<T, MULTI>(o, sp0, b.scenes, b.pbase, b.n_scenes);
-  vec4_t<T> P = a.tape[2 * (size_t)o];
-  vec4_t<T> V = a.tape[2 * (size_t)o + 1];
+  const uint32_t p = blockIdx.x * STEP_THREADS + threadIdx.x;
+  if (p >= b.n) return;
+  const SceneParams<T>& sp = scene_of<T, MULTI>(p, sp0, b.scenes, b.pbase, b.n_scenes);
+  const uint32_t o = a.tape.o[p];
+  vec4_t<T> P = a.tape.p[p];
+  vec4_t<T> V = a.tape.v[p];
   integrate<T>(P, V, sp);  // x', v'
   using A = Ar<T>;
   const T r = P.w;
   const T xs[3] = {P.x, P.y, P.z}, vs[3] = {V.x, V.y, V.z};
   const int lo_idx[3] = {PS_XMIN, PS_YMIN, PS_ZMIN}, hi_idx[3] = {PS_XMAX, PS_YMAX, PS_ZMAX};
-  double* acc = a.acc + o;  // row c at acc[c * n]
+  double* acc = a.acc + p;  // row c at acc[c * n]
   const vec4_t<T> X2 = a.ax2[o], V2 = a.av2[o];
   const T xb2[3] = {X2.x, X2.y, X2.z}, vb2[3] = {V2.x, V2.y, V2.z};
   T xo[3], vo[3];
@@ -200,24 +212,24 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_walls_integrate(StepBufs<T
   a.av[o] = vw;
 }
 
-// Gather the at-rest state (P0, V1) into the tape row in original order.
+// Copy the at-rest state (P0, V1, orig) into a tape row.
 template <class T>
-__global__ void k_tape_write(StepBufs<T> b, vec4_t<T>* row) {
+__global__ void k_tape_write(StepBufs<T> b, TapeRow<T> row) {
   const uint32_t p = blockIdx.x * STEP_THREADS + threadIdx.x;
   if (p >= b.n) return;
-  const uint32_t o = b.orig[p];
-  row[2 * (size_t)o] = b.P0[p];
-  row[2 * (size_t)o + 1] = b.V1[p];
+  row.p[p] = b.P0[p];
+  row.v[p] = b.V1[p];
+  row.o[p] = b.orig[p];
 }
 
-// Put a tape row back as the at-rest state in original order (orig = id).
+// Put a tape row back as the at-rest state.
 template <class T>
-__global__ void k_tape_read(StepBufs<T> b, const vec4_t<T>* row) {
-  const uint32_t o = blockIdx.x * STEP_THREADS + threadIdx.x;
-  if (o >= b.n) return;
-  b.P0[o] = row[2 * (size_t)o];
-  b.V1[o] = row[2 * (size_t)o + 1];
-  b.orig[o] = o;
+__global__ void k_tape_read(StepBufs<T> b, TapeRow<T> row) {
+  const uint32_t p = blockIdx.x * STEP_THREADS + threadIdx.x;
+  if (p >= b.n) return;
+  b.P0[p] = row.p[p];
+  b.V1[p] = row.v[p];
+  b.orig[p] = row.o[p];
 }
 
 // Per-scene sums of the parameter partials (acc: ADJ_NACC rows of n), in a

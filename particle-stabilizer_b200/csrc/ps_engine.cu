@@ -151,6 +151,9 @@ StepBufs<T> bufs(ps_sim* s) {
   b.scell = s->scell;
   b.bounds = static_cast<const T*>(s->d_bounds);
   b.n_tiles = (uint32_t)scan_num_tiles(n_scan(s));
+  b.tape_p = nullptr;
+  b.tape_v = nullptr;
+  b.tape_o = nullptr;
   return b;
 }
 
@@ -819,10 +822,48 @@ __global__ void k_adj_download(const vec4_t<T>* ax, const vec4_t<T>* av, double*
   q[3] = (double)v.x; q[4] = (double)v.y; q[5] = (double)v.z;
 }
 
+// Tape row t of a block: the at-rest state after t steps, sorted order.
+template <class T>
+TapeRow<T> tape_row(char* base, size_t row_bytes, int64_t n, int64_t t) {
+  TapeRow<T> r;
+  char* p = base + row_bytes * (size_t)t;
+  r.p = reinterpret_cast<vec4_t<T>*>(p);
+  r.v = r.p + n;
+  r.o = reinterpret_cast<uint32_t*>(r.v + n);
+  return r;
+}
+
+// Recompute `steps` steps of a block eagerly (box containers), the contact
+// kernel of step k writing tape row k + 1.
+template <class T, bool MULTI>
+void enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes) {
+  StepBufs<T> b = bufs<T>(s);
+  const SceneParams<T> sp0 = params<T>(s)[0];
+  const unsigned gp = blocks_for(s->n_total);
+  const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
+  cudaStream_t st = s->stream;
+  k_begin<T, MULTI, false, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+  for (int64_t k = 0; k < steps; ++k) {
+    const TapeRow<T> row = tape_row<T>(tape, row_bytes, s->n_total, k + 1);
+    b.tape_p = row.p;
+    b.tape_v = row.v;
+    b.tape_o = row.o;
+    k_scan_with_tile_sums<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->tile_sum);
+    k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
+                                                                         s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
+    k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
+    if (k + 1 < steps)
+      k_contacts<T, MULTI, false, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+    else
+      k_contacts<T, MULTI, false, false><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+  }
+}
+
 template <class T, bool MULTI>
 int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl_dstate0) {
   const int64_t n = s->n_total, K = s->fwd_every;
-  const size_t tape_b = align_up(2 * sizeof(vec4_t<T>) * (size_t)n * (size_t)K, 256);
+  const size_t row_b = align_up((2 * sizeof(vec4_t<T>) + sizeof(uint32_t)) * (size_t)n, 256);
+  const size_t tape_b = row_b * (size_t)K;
   const size_t adj_b = align_up(sizeof(vec4_t<T>) * (size_t)n, 256);
   const size_t acc_b = align_up(ADJ_NACC * sizeof(double) * (size_t)n, 256);
   const size_t io_b = align_up(6 * sizeof(double) * (size_t)n, 256);
@@ -836,10 +877,10 @@ int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl
     s->adj_bytes = need;
   }
   char* p = static_cast<char*>(s->adj_arena);
-  vec4_t<T>* tape = reinterpret_cast<vec4_t<T>*>(p);
+  char* tape = p;
   p += tape_b;
   AdjBufs<T> a;
-  a.tape = tape;
+  a.tape = tape_row<T>(tape, row_b, n, 0);
   a.ax = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
   a.av = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
   a.ax2 = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
@@ -859,17 +900,13 @@ int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl
     const int64_t kb = std::min(K, s->fwd_steps - blk * K);
     int rc = load_state(s, s->fwd_ckpt[(size_t)blk]);
     if (rc != PS_OK) return rc;
-    for (int64_t t = 0; t < kb; ++t) {  // recompute the block, recording each step's input
-      StepBufs<T> b = bufs<T>(s);
-      k_tape_write<T><<<gp, STEP_THREADS, 0, st>>>(b, tape + 2 * (size_t)n * (size_t)t);
-      if (t + 1 < kb) {
-        rc = ps_step(s, 1);
-        if (rc != PS_OK) return rc;
-      }
-    }
+    // recompute the block, recording each step's input (row 0 = block start)
+    k_tape_write<T><<<gp, STEP_THREADS, 0, st>>>(bufs<T>(s), tape_row<T>(tape, row_b, n, 0));
+    if (kb > 1) enqueue_steps_taped<T, MULTI>(s, kb - 1, tape, row_b);
+    PS_CUDA(cudaGetLastError());
     for (int64_t t = kb - 1; t >= 0; --t) {
       StepBufs<T> b = bufs<T>(s);
-      a.tape = tape + 2 * (size_t)n * (size_t)t;
+      a.tape = tape_row<T>(tape, row_b, n, t);
       k_tape_read<T><<<gp, STEP_THREADS, 0, st>>>(b, a.tape);
       enqueue_prepare<T, MULTI>(s);
       k_adj_contacts<T, MULTI><<<gp, STEP_THREADS, 0, st>>>(b, a, sp0);

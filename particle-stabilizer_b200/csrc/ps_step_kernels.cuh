@@ -166,6 +166,11 @@ struct StepBufs {
   uint32_t n_tiles;
   uint32_t* scell;        // global cell id of each sorted slot (written by k_rank_move)
   const T* bounds;        // per-scene, per-axis cell boundaries (see SceneParams::bnd_base)
+  // Optional tape row (null outside the adjoint's recompute): k_contacts
+  // writes the at-rest state after its step, in sorted order.
+  vec4_t<T>* tape_p;
+  vec4_t<T>* tape_v;
+  uint32_t* tape_o;
 };
 
 // Container step + hash + count on an integrated state, shared by k_begin and
@@ -365,6 +370,11 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 5 : 4) k_contac
     V.x = vx;
     V.y = vy;
     V.z = vz;
+    if (b.tape_p != nullptr) {  // the at-rest state after this step
+      b.tape_p[i] = P;
+      b.tape_v[i] = V;
+      b.tape_o[i] = b.orig[i];
+    }
     if (FUSED) {
       integrate<T>(P, V, sp);
       if constexpr (MESH) {

@@ -30,10 +30,12 @@ STEPS = int(G["steps"])
 SLAB = tuple(float(x) for x in G["slab"])
 HIST_TOP = float(G["hist_top"])
 
-# Tolerances for runs that are not bit-identical to the oracle's FP64 run.
-PACKING_TOL = 0.01   # absolute, on a packing fraction of about 0.5
-HIST_TV_TOL = 0.06   # total-variation distance between height histograms
-ZMEAN_TOL = 0.01     # relative, on the mean centre height
+# Tolerances for runs that are not bit-identical to the oracle's FP64 run,
+# about five times the differences measured on a B200 (FP32: 2e-5, 0.012,
+# 4e-4; reference CUDA build: 5.4e-4, 0.015, 7e-5).
+PACKING_TOL = 0.003  # absolute, on a slab packing fraction of 0.613
+HIST_TV_TOL = 0.06   # total-variation distance between height histograms (24 bins)
+ZMEAN_TOL = 0.002    # relative, on the mean centre height
 
 
 def summary(sc, state):
