@@ -17,10 +17,13 @@
 //   k_adj_walls_integrate (the tape row's sorted order): through the walls
 //                    (clamp events recomputed from the recorded step input)
 //                    and the integrate; partials of dL/de_wall by slot.
-// The tape holds each step's input as the at-rest state in sorted order
-// (positions, velocities, original ids): rows are written and read with
-// coalesced accesses, and replaying a step starts from a spatially sorted
-// state, so its hash-and-count pass aggregates its atomics.
+// The block recompute records, per step, the at-rest state after it in
+// sorted order (positions, velocities, original ids) together with the
+// step's grid (pre-contact velocities, sorted cell ids, and a copy of the
+// cell offsets).  Row t + 1 plus offsets t are then exactly the sorted
+// post-wall state and grid that step t's contacts read, so the reverse sweep
+// runs the contact adjoint on them directly, without rebuilding the grid,
+// and row t is the step's input for the walls/integrate adjoint.
 // Wall clamps and contact activation are piecewise events taken from the
 // forward values; radii and masses are constants.
 #pragma once
@@ -34,9 +37,11 @@ constexpr int ADJ_NACC = 8;
 
 template <class T>
 struct TapeRow {
-  vec4_t<T>* p;  // (x, r) per sorted slot
-  vec4_t<T>* v;  // (v, m)
-  uint32_t* o;   // original id
+  vec4_t<T>* p;     // (x, r) per sorted slot
+  vec4_t<T>* v;     // (v, m)
+  vec4_t<T>* vpre;  // (v, m) before the contacts of the step that wrote the row
+  uint32_t* o;      // original id
+  uint32_t* cell;   // sorted cell id of that step's grid
 };
 
 template <class T>
@@ -222,15 +227,6 @@ __global__ void k_tape_write(StepBufs<T> b, TapeRow<T> row) {
   row.o[p] = b.orig[p];
 }
 
-// Put a tape row back as the at-rest state.
-template <class T>
-__global__ void k_tape_read(StepBufs<T> b, TapeRow<T> row) {
-  const uint32_t p = blockIdx.x * STEP_THREADS + threadIdx.x;
-  if (p >= b.n) return;
-  b.P0[p] = row.p[p];
-  b.V1[p] = row.v[p];
-  b.orig[p] = row.o[p];
-}
 
 // Per-scene sums of the parameter partials (acc: ADJ_NACC rows of n), in a
 // fixed order.

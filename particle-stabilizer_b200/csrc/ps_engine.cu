@@ -153,7 +153,9 @@ StepBufs<T> bufs(ps_sim* s) {
   b.n_tiles = (uint32_t)scan_num_tiles(n_scan(s));
   b.tape_p = nullptr;
   b.tape_v = nullptr;
+  b.tape_vpre = nullptr;
   b.tape_o = nullptr;
+  b.tape_cell = nullptr;
   return b;
 }
 
@@ -784,22 +786,6 @@ int load_state(ps_sim* s, const void* buf) {
   return PS_OK;
 }
 
-// integrate + walls + grid of the at-rest state, leaving the sorted post-wall
-// state in (P0, V0) for the contact adjoint (the first half of a step)
-template <class T, bool MULTI>
-void enqueue_prepare(ps_sim* s) {
-  const StepBufs<T> b = bufs<T>(s);
-  const SceneParams<T> sp0 = params<T>(s)[0];
-  const unsigned gp = blocks_for(s->n_total);
-  cudaStream_t st = s->stream;
-  k_begin<T, MULTI, false, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
-  k_scan_with_tile_sums<<<(unsigned)scan_num_tiles(n_scan(s)), SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s),
-                                                                                     s->tile_sum);
-  k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
-                                                                       s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
-  k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
-}
-
 template <class T>
 __global__ void k_adj_upload(const double* __restrict__ g, vec4_t<T>* ax, vec4_t<T>* av, uint32_t n) {
   const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
@@ -822,21 +808,29 @@ __global__ void k_adj_download(const vec4_t<T>* ax, const vec4_t<T>* av, double*
   q[3] = (double)v.x; q[4] = (double)v.y; q[5] = (double)v.z;
 }
 
-// Tape row t of a block: the at-rest state after t steps, sorted order.
+// Tape row t of a block: the at-rest state after t steps in sorted order;
+// rows t >= 1 also hold step t-1's grid (pre-contact velocities, cell ids).
 template <class T>
 TapeRow<T> tape_row(char* base, size_t row_bytes, int64_t n, int64_t t) {
   TapeRow<T> r;
   char* p = base + row_bytes * (size_t)t;
   r.p = reinterpret_cast<vec4_t<T>*>(p);
   r.v = r.p + n;
-  r.o = reinterpret_cast<uint32_t*>(r.v + n);
+  r.vpre = r.v + n;
+  r.o = reinterpret_cast<uint32_t*>(r.vpre + n);
+  r.cell = r.o + n;
   return r;
 }
 
-// Recompute `steps` steps of a block eagerly (box containers), the contact
-// kernel of step k writing tape row k + 1.
+size_t tape_row_bytes(size_t vec_bytes, int64_t n) {
+  return align_up((3 * vec_bytes + 2 * sizeof(uint32_t)) * (size_t)n, 256);
+}
+
+// Recompute `steps` steps of a block eagerly (box containers): step k's
+// contact kernel writes tape row k + 1 and its cell offsets are copied to
+// offsets slot k.
 template <class T, bool MULTI>
-void enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes) {
+int enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes, uint32_t* offs, size_t offs_stride) {
   StepBufs<T> b = bufs<T>(s);
   const SceneParams<T> sp0 = params<T>(s)[0];
   const unsigned gp = blocks_for(s->n_total);
@@ -852,23 +846,30 @@ void enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes)
     k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
                                                                          s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
     k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
+    b.tape_vpre = row.vpre;
+    b.tape_cell = row.cell;
+    PS_CUDA(cudaMemcpyAsync(offs + offs_stride * (size_t)k, s->offset, sizeof(uint32_t) * (size_t)n_scan(s),
+                            cudaMemcpyDeviceToDevice, st));
     if (k + 1 < steps)
       k_contacts<T, MULTI, false, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
     else
       k_contacts<T, MULTI, false, false><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
   }
+  return PS_OK;
 }
 
 template <class T, bool MULTI>
 int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl_dstate0) {
   const int64_t n = s->n_total, K = s->fwd_every;
-  const size_t row_b = align_up((2 * sizeof(vec4_t<T>) + sizeof(uint32_t)) * (size_t)n, 256);
-  const size_t tape_b = row_b * (size_t)K;
+  const size_t row_b = tape_row_bytes(sizeof(vec4_t<T>), n);
+  const size_t tape_b = row_b * (size_t)(K + 1);                 // rows 0..K
+  const size_t offs_stride = align_up(sizeof(uint32_t) * (size_t)n_scan(s), 256) / sizeof(uint32_t);
+  const size_t offs_b = sizeof(uint32_t) * offs_stride * (size_t)K;  // cell offsets of each step's grid
   const size_t adj_b = align_up(sizeof(vec4_t<T>) * (size_t)n, 256);
   const size_t acc_b = align_up(ADJ_NACC * sizeof(double) * (size_t)n, 256);
   const size_t io_b = align_up(6 * sizeof(double) * (size_t)n, 256);
   const size_t red_b = align_up(ADJ_NACC * sizeof(double) * (size_t)s->n_scenes, 256);
-  const size_t need = tape_b + 4 * adj_b + acc_b + io_b + red_b;
+  const size_t need = tape_b + offs_b + 4 * adj_b + acc_b + io_b + red_b;
   if (s->adj_bytes < need) {
     cudaFree(s->adj_arena);
     s->adj_arena = nullptr;
@@ -879,6 +880,8 @@ int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl
   char* p = static_cast<char*>(s->adj_arena);
   char* tape = p;
   p += tape_b;
+  uint32_t* offs = reinterpret_cast<uint32_t*>(p);
+  p += offs_b;
   AdjBufs<T> a;
   a.tape = tape_row<T>(tape, row_b, n, 0);
   a.ax = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
@@ -900,15 +903,21 @@ int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl
     const int64_t kb = std::min(K, s->fwd_steps - blk * K);
     int rc = load_state(s, s->fwd_ckpt[(size_t)blk]);
     if (rc != PS_OK) return rc;
-    // recompute the block, recording each step's input (row 0 = block start)
+    // recompute the block, recording each step's input and grid (row 0 = block start)
     k_tape_write<T><<<gp, STEP_THREADS, 0, st>>>(bufs<T>(s), tape_row<T>(tape, row_b, n, 0));
-    if (kb > 1) enqueue_steps_taped<T, MULTI>(s, kb - 1, tape, row_b);
+    rc = enqueue_steps_taped<T, MULTI>(s, kb, tape, row_b, offs, offs_stride);
+    if (rc != PS_OK) return rc;
     PS_CUDA(cudaGetLastError());
     for (int64_t t = kb - 1; t >= 0; --t) {
+      // step t's sorted post-wall state and grid: row t + 1 and offsets t
+      const TapeRow<T> g = tape_row<T>(tape, row_b, n, t + 1);
       StepBufs<T> b = bufs<T>(s);
+      b.P0 = g.p;
+      b.V0 = g.vpre;
+      b.orig = g.o;
+      b.scell = g.cell;
+      b.offset = offs + offs_stride * (size_t)t;
       a.tape = tape_row<T>(tape, row_b, n, t);
-      k_tape_read<T><<<gp, STEP_THREADS, 0, st>>>(b, a.tape);
-      enqueue_prepare<T, MULTI>(s);
       k_adj_contacts<T, MULTI><<<gp, STEP_THREADS, 0, st>>>(b, a, sp0);
       k_adj_walls_integrate<T, MULTI><<<gp, STEP_THREADS, 0, st>>>(b, a, sp0);
       PS_CUDA(cudaGetLastError());

@@ -167,10 +167,13 @@ struct StepBufs {
   uint32_t* scell;        // global cell id of each sorted slot (written by k_rank_move)
   const T* bounds;        // per-scene, per-axis cell boundaries (see SceneParams::bnd_base)
   // Optional tape row (null outside the adjoint's recompute): k_contacts
-  // writes the at-rest state after its step, in sorted order.
+  // writes the at-rest state after its step in sorted order, and the
+  // pre-contact velocity and sorted cell id of the step's grid.
   vec4_t<T>* tape_p;
   vec4_t<T>* tape_v;
+  vec4_t<T>* tape_vpre;
   uint32_t* tape_o;
+  uint32_t* tape_cell;
 };
 
 // Container step + hash + count on an integrated state, shared by k_begin and
@@ -370,10 +373,12 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 5 : 4) k_contac
     V.x = vx;
     V.y = vy;
     V.z = vz;
-    if (b.tape_p != nullptr) {  // the at-rest state after this step
+    if (b.tape_p != nullptr) {  // the at-rest state after this step, and this step's grid
       b.tape_p[i] = P;
       b.tape_v[i] = V;
+      b.tape_vpre[i] = Vi;
       b.tape_o[i] = b.orig[i];
+      b.tape_cell[i] = b.scell[i];
     }
     if (FUSED) {
       integrate<T>(P, V, sp);
