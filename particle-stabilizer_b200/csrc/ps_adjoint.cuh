@@ -56,31 +56,39 @@ struct AdjBufs {
   uint32_t n;             // row length of acc
 };
 
-// Terms of one active pair for the receiver r and the source s:
-// c_r = f d; g = adjoint of v_r's output.  Returns the adjoint of d (dd),
-// of u (du) and the parameter partials.
+// Geometry of one active pair, shared by its two directions: d = x_i - x_j,
+// u = v_i - v_j, L = |d|, ov = R - L, ud = u.d, and the reciprocals.
 template <class T>
-__device__ __forceinline__ void pair_adjoint(T dx, T dy, T dz, T ux, T uy, T uz, T R, T mr, T ms, T k, T e, T gx,
+struct PairGeom {
+  T dx, dy, dz, ux, uy, uz, L, iL, iL2, ov, ud, R;
+};
+
+// Terms of one direction of an active pair for the receiver r and the
+// source s: c_r = f d with f = k ov / (L m_r) - B ud / L^2,
+// B = 2 m_s e / (m_r + m_s); g = adjoint of v_r's output; sgn = +1 when r is
+// the pair's first sphere (d as stored) and -1 when it is the second (d and
+// u negated, ud and L unchanged).  Returns the adjoint of d and of u with
+// respect to the pair's stored d and u, and adds the parameter partials.
+template <class T>
+__device__ __forceinline__ void pair_adjoint(const PairGeom<T>& q, T sgn, T mr, T ms, T inv_msum, T k, T e, T gx,
                                              T gy, T gz, T& ddx, T& ddy, T& ddz, T& dux, T& duy, T& duz,
                                              double& dk, double& de) {
-  const T L2 = dx * dx + dy * dy + dz * dz;
-  const T L = sqrt(L2);
-  const T ov = R - L;
-  const T Bc = T(2) * ms * e / (mr + ms);
-  const T ud = ux * dx + uy * dy + uz * dz;
-  const T f = k * ov / (L * mr) - Bc * ud / L2;
-  const T fbar = gx * dx + gy * dy + gz * dz;
-  dk += (double)(fbar * ov / (L * mr));
-  de += (double)(fbar * (-(T(2) * ms * ud) / ((mr + ms) * L2)));
-  const T fL = -k * R / (L2 * mr) + T(2) * Bc * ud / (L2 * L);
-  const T Lb = fbar * fL / L;
-  const T udb = -fbar * Bc / L2;
-  ddx = f * gx + Lb * dx + udb * ux;
-  ddy = f * gy + Lb * dy + udb * uy;
-  ddz = f * gz + Lb * dz + udb * uz;
-  dux = udb * dx;
-  duy = udb * dy;
-  duz = udb * dz;
+  const T imr = T(1) / mr;
+  const T Bc = T(2) * ms * e * inv_msum;
+  const T f = k * q.ov * q.iL * imr - Bc * q.ud * q.iL2;
+  const T fbar = sgn * (gx * q.dx + gy * q.dy + gz * q.dz);
+  dk += (double)(fbar * q.ov * q.iL * imr);
+  de += (double)(fbar * (-(T(2) * ms * q.ud) * inv_msum * q.iL2));
+  const T fL = -k * q.R * q.iL2 * imr + T(2) * Bc * q.ud * q.iL2 * q.iL;
+  const T Lb = fbar * fL * q.iL;
+  const T udb = -fbar * Bc * q.iL2;
+  // adjoint of the direction's own d (= sgn d) and u (= sgn u), mapped back
+  ddx = sgn * (f * gx) + Lb * q.dx + udb * q.ux;
+  ddy = sgn * (f * gy) + Lb * q.dy + udb * q.uy;
+  ddz = sgn * (f * gz) + Lb * q.dz + udb * q.uz;
+  dux = udb * q.dx;
+  duy = udb * q.dy;
+  duz = udb * q.dz;
 }
 
 // Same activation test as the forward contact kernel (contact_one).
@@ -115,43 +123,60 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, Ad
   const uint32_t z1 = (uint32_t)(cz + 1 < nz ? cz + 1 : nz - 1) + 1u;
   const T k = sp.k_spring, e = sp.e_sphere;
   const bool live = isfinite(P.x) && isfinite(P.y) && isfinite(P.z);  // no active pair otherwise
-  for (int q = 0; q < 9; ++q) {
+  uint32_t lo[9], hi[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {  // the 18 range bounds, loaded together
     const int32_t bx = cx - 1 + q / 3, by = cy - 1 + q % 3;
-    if (!live || bx < 0 || bx >= nx || by < 0 || by >= ny) continue;
-    const uint32_t col = sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz;
-    const uint32_t j0 = b.offset[col + z0], j1 = b.offset[col + z1];
-    for (uint32_t j = j0; j < j1; ++j) {
+    const bool ok = live && bx >= 0 && bx < nx && by >= 0 && by < ny;
+    const uint32_t col = ok ? sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz : sp.cbase;
+    lo[q] = ok ? __ldg(b.offset + col + z0) : 0u;
+    hi[q] = ok ? __ldg(b.offset + col + z1) : 0u;
+  }
+#pragma unroll
+  for (int q = 0; q < 9; ++q)
+    for (uint32_t j = lo[q]; j < hi[q]; ++j) {
       if (j == i) continue;
-      const vec4_t<T> Pj = b.P0[j];
+      const vec4_t<T> Pj = ld4<T>(b.P0 + j);
       if (!pair_active<T>(P, Pj)) continue;
       const vec4_t<T> Vj = b.V0[j];
       const uint32_t oj = b.orig[j];
-      const T dx = P.x - Pj.x, dy = P.y - Pj.y, dz = P.z - Pj.z;
-      const T ux = V.x - Vj.x, uy = V.y - Vj.y, uz = V.z - Vj.z;
-      const T R = P.w + Pj.w;
+      const vec4_t<T> H = a.av[oj];
+      PairGeom<T> g;
+      g.dx = P.x - Pj.x;
+      g.dy = P.y - Pj.y;
+      g.dz = P.z - Pj.z;
+      g.ux = V.x - Vj.x;
+      g.uy = V.y - Vj.y;
+      g.uz = V.z - Vj.z;
+      g.R = P.w + Pj.w;
+      const T L2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz;
+      g.L = sqrt(L2);
+      g.iL = T(1) / g.L;
+      g.iL2 = T(1) / L2;
+      g.ov = g.R - g.L;
+      g.ud = g.ux * g.dx + g.uy * g.dy + g.uz * g.dz;
+      const T inv_msum = T(1) / (V.w + Vj.w);
       T ddx, ddy, ddz, dux, duy, duz;
       // i receives from j
-      pair_adjoint<T>(dx, dy, dz, ux, uy, uz, R, V.w, Vj.w, k, e, gx, gy, gz, ddx, ddy, ddz, dux, duy, duz, dk, de);
+      pair_adjoint<T>(g, T(1), V.w, Vj.w, inv_msum, k, e, gx, gy, gz, ddx, ddy, ddz, dux, duy, duz, dk, de);
       xb0 += ddx;
       xb1 += ddy;
       xb2 += ddz;
       vb0 += dux;
       vb1 += duy;
       vb2 += duz;
-      // j receives from i: i enters as the source (d and u change sign)
+      // j receives from i: that direction's d and u are -d and -u, so its
+      // adjoints with respect to the stored d and u come back sign-mapped;
+      // its parameter partials belong to j's own thread
       double dk2 = 0.0, de2 = 0.0;
-      const vec4_t<T> H = a.av[oj];
-      const T hx = H.x, hy = H.y, hz = H.z;
-      pair_adjoint<T>(-dx, -dy, -dz, -ux, -uy, -uz, R, Vj.w, V.w, k, e, hx, hy, hz, ddx, ddy, ddz, dux, duy, duz, dk2,
-                      de2);
-      xb0 -= ddx;
-      xb1 -= ddy;
-      xb2 -= ddz;
-      vb0 -= dux;
-      vb1 -= duy;
-      vb2 -= duz;
+      pair_adjoint<T>(g, T(-1), Vj.w, V.w, inv_msum, k, e, H.x, H.y, H.z, ddx, ddy, ddz, dux, duy, duz, dk2, de2);
+      xb0 += ddx;
+      xb1 += ddy;
+      xb2 += ddz;
+      vb0 += dux;
+      vb1 += duy;
+      vb2 += duz;
     }
-  }
   vec4_t<T> xo = X, vo = G;
   xo.x = xb0;
   xo.y = xb1;
