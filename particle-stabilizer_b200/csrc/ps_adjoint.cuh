@@ -47,10 +47,16 @@ struct TapeRow {
 template <class T>
 struct AdjBufs {
   TapeRow<T> tape;        // input of the step being reversed
-  vec4_t<T>* ax;          // adjoint of positions, original order (w unused): one 16/32-B access
-  vec4_t<T>* av;          // adjoint of velocities
-  vec4_t<T>* ax2;         // output of k_adj_contacts
+  // Adjoints of positions and velocities (w unused), one 16/32-B record per
+  // particle, kept in the sorted order of the at-rest state they belong to:
+  // before step t's reverse they follow the order after step t (its grid's
+  // order), after it the order of step t's input (the previous grid's), so
+  // every kernel reads and writes them by slot.
+  vec4_t<T>* ax;
+  vec4_t<T>* av;
+  vec4_t<T>* ax2;         // output of k_adj_contacts, in the order of step t's grid
   vec4_t<T>* av2;
+  uint32_t* inv;          // slot in step t's grid of each original id (written by k_adj_contacts)
   double* acc;            // ADJ_NACC rows of n, accumulated over steps: rows k, e by sorted
                           // slot, wall rows by original index
   uint32_t n;             // row length of acc
@@ -111,7 +117,8 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, Ad
   const vec4_t<T> P = b.P0[i];
   const vec4_t<T> V = b.V0[i];
   const uint32_t oi = b.orig[i];
-  const vec4_t<T> G = a.av[oi], X = a.ax[oi];
+  a.inv[oi] = i;
+  const vec4_t<T> G = a.av[i], X = a.ax[i];
   const T gx = G.x, gy = G.y, gz = G.z;
   T xb0 = X.x, xb1 = X.y, xb2 = X.z;
   T vb0 = gx, vb1 = gy, vb2 = gz;
@@ -139,8 +146,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, Ad
       const vec4_t<T> Pj = ld4<T>(b.P0 + j);
       if (!pair_active<T>(P, Pj)) continue;
       const vec4_t<T> Vj = b.V0[j];
-      const uint32_t oj = b.orig[j];
-      const vec4_t<T> H = a.av[oj];
+      const vec4_t<T> H = a.av[j];
       PairGeom<T> g;
       g.dx = P.x - Pj.x;
       g.dy = P.y - Pj.y;
@@ -184,8 +190,8 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, Ad
   vo.x = vb0;
   vo.y = vb1;
   vo.z = vb2;
-  a.ax2[oi] = xo;
-  a.av2[oi] = vo;
+  a.ax2[i] = xo;
+  a.av2[i] = vo;
   a.acc[(size_t)ADJ_K * a.n + i] += dk;
   a.acc[(size_t)ADJ_E * a.n + i] += de;
 }
@@ -208,7 +214,8 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_walls_integrate(StepBufs<T
   const T xs[3] = {P.x, P.y, P.z}, vs[3] = {V.x, V.y, V.z};
   const int lo_idx[3] = {PS_XMIN, PS_YMIN, PS_ZMIN}, hi_idx[3] = {PS_XMAX, PS_YMAX, PS_ZMAX};
   double* acc = a.acc + p;  // row c at acc[c * n]
-  const vec4_t<T> X2 = a.ax2[o], V2 = a.av2[o];
+  const uint32_t i = a.inv[o];  // this particle's slot in step t's grid
+  const vec4_t<T> X2 = a.ax2[i], V2 = a.av2[i];
   const T xb2[3] = {X2.x, X2.y, X2.z}, vb2[3] = {V2.x, V2.y, V2.z};
   T xo[3], vo[3];
 #pragma unroll
@@ -238,8 +245,8 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_walls_integrate(StepBufs<T
   vw.x = vo[0];
   vw.y = vo[1];
   vw.z = vo[2];
-  a.ax[o] = xw;
-  a.av[o] = vw;
+  a.ax[p] = xw;
+  a.av[p] = vw;
 }
 
 // Copy the at-rest state (P0, V1, orig) into a tape row.

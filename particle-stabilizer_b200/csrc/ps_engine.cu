@@ -786,11 +786,13 @@ int load_state(ps_sim* s, const void* buf) {
   return PS_OK;
 }
 
+// dL/d(final state), original order, gathered into the final state's sorted order.
 template <class T>
-__global__ void k_adj_upload(const double* __restrict__ g, vec4_t<T>* ax, vec4_t<T>* av, uint32_t n) {
+__global__ void k_adj_upload(const double* __restrict__ g, const uint32_t* __restrict__ orig, vec4_t<T>* ax,
+                             vec4_t<T>* av, uint32_t n) {
   const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= n) return;
-  const double* q = g + 6 * (size_t)o;
+  const double* q = g + 6 * (size_t)orig[o];
   vec4_t<T> x, v;
   x.x = (T)q[0]; x.y = (T)q[1]; x.z = (T)q[2]; x.w = T(0);
   v.x = (T)q[3]; v.y = (T)q[4]; v.z = (T)q[5]; v.w = T(0);
@@ -798,12 +800,14 @@ __global__ void k_adj_upload(const double* __restrict__ g, vec4_t<T>* ax, vec4_t
   av[o] = v;
 }
 
+// dL/d(initial state) from the initial state's sorted order back to original order.
 template <class T>
-__global__ void k_adj_download(const vec4_t<T>* ax, const vec4_t<T>* av, double* __restrict__ g, uint32_t n) {
+__global__ void k_adj_download(const vec4_t<T>* ax, const vec4_t<T>* av, const uint32_t* __restrict__ orig,
+                               double* __restrict__ g, uint32_t n) {
   const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= n) return;
   const vec4_t<T> x = ax[o], v = av[o];
-  double* q = g + 6 * (size_t)o;
+  double* q = g + 6 * (size_t)orig[o];
   q[0] = (double)x.x; q[1] = (double)x.y; q[2] = (double)x.z;
   q[3] = (double)v.x; q[4] = (double)v.y; q[5] = (double)v.z;
 }
@@ -869,7 +873,8 @@ int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl
   const size_t acc_b = align_up(ADJ_NACC * sizeof(double) * (size_t)n, 256);
   const size_t io_b = align_up(6 * sizeof(double) * (size_t)n, 256);
   const size_t red_b = align_up(ADJ_NACC * sizeof(double) * (size_t)s->n_scenes, 256);
-  const size_t need = tape_b + offs_b + 4 * adj_b + acc_b + io_b + red_b;
+  const size_t inv_b = align_up(sizeof(uint32_t) * (size_t)n, 256);
+  const size_t need = tape_b + offs_b + 4 * adj_b + inv_b + acc_b + io_b + red_b;
   if (s->adj_bytes < need) {
     cudaFree(s->adj_arena);
     s->adj_arena = nullptr;
@@ -888,14 +893,18 @@ int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl
   a.av = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
   a.ax2 = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
   a.av2 = reinterpret_cast<vec4_t<T>*>(p); p += adj_b;
+  a.inv = reinterpret_cast<uint32_t*>(p); p += inv_b;
   a.acc = reinterpret_cast<double*>(p); p += acc_b;
   a.n = (uint32_t)n;
   double* io = reinterpret_cast<double*>(p); p += io_b;
   double* red = reinterpret_cast<double*>(p);
   cudaStream_t st = s->stream;
   const unsigned gp = blocks_for(n);
+  // the final state's order (recomputing the last block reproduces it exactly)
+  int rc0 = load_state(s, s->fwd_ckpt.back());
+  if (rc0 != PS_OK) return rc0;
   PS_CUDA(cudaMemcpyAsync(io, dl_dstate, 6 * sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, st));
-  k_adj_upload<T><<<gp, STEP_THREADS, 0, st>>>(io, a.ax, a.av, (uint32_t)n);
+  k_adj_upload<T><<<gp, STEP_THREADS, 0, st>>>(io, s->orig, a.ax, a.av, (uint32_t)n);
   PS_CUDA(cudaMemsetAsync(a.acc, 0, acc_b, st));
   const SceneParams<T> sp0 = params<T>(s)[0];
   const int64_t n_blocks = (s->fwd_steps + K - 1) / K;
@@ -927,7 +936,8 @@ int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl
   std::vector<double> h((size_t)ADJ_NACC * s->n_scenes);
   PS_CUDA(cudaMemcpyAsync(h.data(), red, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
   if (dl_dstate0 != nullptr) {
-    k_adj_download<T><<<gp, STEP_THREADS, 0, st>>>(a.ax, a.av, io, (uint32_t)n);
+    // block 0's row 0 is the initial state, in the order the adjoints now follow
+    k_adj_download<T><<<gp, STEP_THREADS, 0, st>>>(a.ax, a.av, tape_row<T>(tape, row_b, n, 0).o, io, (uint32_t)n);
     PS_CUDA(cudaMemcpyAsync(dl_dstate0, io, 6 * sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, st));
   }
   PS_CUDA(cudaStreamSynchronize(st));
