@@ -244,7 +244,7 @@ def adjoint_measure(psb200, sc, steps, every, device, restore_block=None) -> dic
 
 
 def batch_measure(psb200, scenes_mod, device, steps: int, n_scenes: int, sequential: bool = True,
-                  k_range=(5e3, 5e4)) -> dict:
+                  k_range=(5e3, 5e4), tune: bool = False) -> dict:
     """256 uneven independent scenes: one simulation advancing all of them per
     launch, against the same scenes run one after another, each as its own
     simulation (steps from each scene's initial state, FP32)."""
@@ -258,11 +258,27 @@ def batch_measure(psb200, scenes_mod, device, steps: int, n_scenes: int, sequent
         batched_ms = sim.time_steps(steps)
         launches = sim.launches()
         bad = non_finite(sim.get_state())
+        tuned = None
+        if tune:
+            # cell size and graph block chosen by ps_autotune, then the same steps again
+            sim.checkpoint_load(0)
+            choice = sim.autotune(trial_steps=20)
+            sim.checkpoint_load(0)
+            sim.time_steps(steps)
+            sim.checkpoint_load(0)
+            tuned_ms = sim.time_steps(steps)
+            tuned = {"batched_ms": tuned_ms, "cell_factor": choice["cell_factor"],
+                     "graph_block": choice["graph_block"], "trial_ms_table": choice["ms_table"],
+                     "trial_cell_factors": choice["cell_factors"], "trial_graph_blocks": choice["graph_blocks"],
+                     "batched_particle_steps_per_s": n_total * steps / (tuned_ms * 1e-3),
+                     "non_finite_at_end": non_finite(sim.get_state())}
     out = {"n_scenes": n_scenes, "n_particles": n_total, "k_range": list(k_range), "steps": steps,
            "batched_ms": batched_ms,
            "batched_scene_steps_per_s": n_scenes * steps / (batched_ms * 1e-3),
            "batched_particle_steps_per_s": n_total * steps / (batched_ms * 1e-3),
            "launches_batched": launches, "non_finite_at_end": bad}
+    if tuned is not None:
+        out["autotuned"] = tuned
     if not sequential:
         return out
     seq_ms = 0.0
@@ -277,6 +293,8 @@ def batch_measure(psb200, scenes_mod, device, steps: int, n_scenes: int, sequent
             seq_launches += s1.launches()
     out.update({"sequential_ms": seq_ms, "sequential_scene_steps_per_s": n_scenes * steps / (seq_ms * 1e-3),
                 "speedup_batched_over_sequential": seq_ms / batched_ms, "launches_sequential": seq_launches})
+    if "autotuned" in out:
+        out["autotuned"]["speedup_over_sequential"] = seq_ms / out["autotuned"]["batched_ms"]
     return out
 
 
@@ -314,7 +332,7 @@ EXTRAS = {
     "adjoint_1m": lambda p, s, dev, a: adjoint_measure(p, s.c4_scene(1 << 20, edge=0.95, k_spring=5.0), 2000, 100,
                                                        dev),
     "batch": lambda p, s, dev, a: batch_measure(p, s, dev, 100, 256, sequential=not a.no_sequential,
-                                                k_range=(0.25, 2.5)),
+                                                k_range=(0.25, 2.5), tune=True),
     "batch_as_specified": lambda p, s, dev, a: batch_measure(p, s, dev, 100, 256, sequential=not a.no_sequential),
     "mesh": lambda p, s, dev, a: mesh_measure(p, s, dev, 20000),
 }

@@ -184,6 +184,28 @@ typedef struct ps_grad {
 int ps_forward_checkpointed(ps_sim* sim, int64_t n_steps, int64_t checkpoint_every);
 int ps_backward(ps_sim* sim, const double* dl_dstate, ps_grad* grads, double* dl_dstate0);
 
+/* ---- autotuning (no counterpart in the reference, whose cell edge is fixed
+ * at 2.1 r_max, ParticleModelCUDA.cpp:84, and which has no step graphs) ----
+ * ps_autotune times `trial_steps` steps from the current state for every
+ * pair of a cell-size factor f (each scene's cell edge becomes f * 2 * r_max
+ * of that scene; f >= 1) and a graph block length L (steps per captured CUDA
+ * graph), keeps the fastest pair, and restores the state.  ms_table (may be
+ * NULL) receives n_factors x n_blocks milliseconds per step, factor-major.
+ * The cell size changes the grid and with it the summation order of the
+ * contacts, so later trajectories are those of the chosen grid: deterministic,
+ * and equal to the oracle's with that cell size, but not bit-equal to runs
+ * with the previous grid.  A recorded ps_forward_checkpointed is dropped.
+ * Allocates device memory (grids, graphs, one state copy). */
+typedef struct ps_tune_result {
+  double cell_factor;        /* chosen f                                          */
+  int64_t graph_block;       /* chosen L                                          */
+  double ms_per_step;        /* trial time per step with the choice               */
+  double before_ms_per_step; /* trial time per step with the grid and L in effect */
+                             /* when ps_autotune was called                       */
+} ps_tune_result;
+int ps_autotune(ps_sim* sim, int64_t trial_steps, const double* cell_factors, int32_t n_factors,
+                const int64_t* graph_blocks, int32_t n_blocks, double* ms_table, ps_tune_result* out);
+
 /* runSimulateCUDA with POD arguments: create, upload, max_steps steps,
  * download, destroy.  aos_out may alias aos_in. */
 int ps_simulate(const ps_scene_desc* scene, const double* aos_in, double* aos_out, int64_t max_steps,

@@ -112,6 +112,7 @@ struct ps_sim {
   std::vector<SceneParams<double>> sp64;
 
   std::map<int64_t, cudaGraphExec_t> graphs;
+  int64_t graph_block = 200;  // steps per captured CUDA graph (ps_autotune may change it)
   int64_t last_launches = 0;
   std::map<int32_t, void*> checkpoints;  // slot -> device copy of (P0, V1, orig)
   cudaAccessPolicyWindow l2_window{};     // count + offset arrays kept in L2
@@ -125,7 +126,6 @@ struct ps_sim {
 
 namespace {
 
-constexpr int64_t kGraphBlock = 200;  // steps per captured graph
 
 int64_t n_scan(const ps_sim* s) { return s->c_total + 1; }
 
@@ -1086,7 +1086,7 @@ extern "C" int ps_step(ps_sim* s, int64_t n_steps) {
   DeviceGuard guard(s->device);
   int64_t left = n_steps;
   while (left > 0) {
-    const int64_t L = std::min(left, kGraphBlock);
+    const int64_t L = std::min(left, s->graph_block);
     auto it = s->graphs.find(L);
     if (it == s->graphs.end()) {
       cudaGraph_t graph = nullptr;
@@ -1160,6 +1160,118 @@ extern "C" int ps_time_steps(ps_sim* s, int64_t n_steps, double* device_ms) {
   if (rc != PS_OK) return rc;
   *device_ms = (double)ms;
   return check_device_error(s);
+}
+
+namespace {
+
+// Rebuild every grid-dependent buffer after the scenes' cell sizes changed.
+// The particle arrays, the state and the checkpoints are kept; the captured
+// step graphs, the adjoint arena and the recorded forward pass are dropped.
+int resize_grids(ps_sim* s, const std::vector<double>& host_state) {
+  for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+  void** bufs_to_free[] = {&s->cell_arena, &s->d_scenes, &s->d_bounds, &s->d_tri, &s->d_nrm, &s->d_aabb,
+                           &s->adj_arena};
+  for (void** b : bufs_to_free) {
+    cudaFree(*b);
+    *b = nullptr;
+  }
+  cudaFree(s->d_bin_offset);
+  cudaFree(s->d_bin_tri);
+  cudaFree(s->d_mesh_view);
+  s->d_bin_offset = s->d_bin_tri = nullptr;
+  s->d_mesh_view = nullptr;
+  s->adj_bytes = 0;
+  s->fwd_steps = 0;
+  s->l2_window_on = false;
+  s->grid_sized = false;
+  s->grid_valid = false;
+  return size_grids(s, host_state.data());
+}
+
+}  // namespace
+
+extern "C" int ps_autotune(ps_sim* s, int64_t trial_steps, const double* cell_factors, int32_t n_factors,
+                           const int64_t* graph_blocks, int32_t n_blocks, double* ms_table, ps_tune_result* out) {
+  if (s == nullptr || out == nullptr || trial_steps < 1 || cell_factors == nullptr || n_factors < 1 ||
+      graph_blocks == nullptr || n_blocks < 1)
+    return fail(PS_ERR_INVALID, "ps_autotune: bad argument");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_autotune: call ps_set_state first");
+  for (int32_t f = 0; f < n_factors; ++f)
+    if (!(cell_factors[f] >= 1.0) || !std::isfinite(cell_factors[f]))
+      return fail(PS_ERR_INVALID, "ps_autotune: cell factors must be finite and >= 1");
+  for (int32_t l = 0; l < n_blocks; ++l)
+    if (graph_blocks[l] < 1) return fail(PS_ERR_INVALID, "ps_autotune: graph blocks must be >= 1");
+  DeviceGuard guard(s->device);
+  // the starting state, on the host (radii for the cell sizes) and on the device
+  std::vector<double> host((size_t)8 * (size_t)std::max<int64_t>(s->n_total, 1));
+  int rc = ps_get_state(s, host.data(), s->n_total);
+  if (rc != PS_OK) return rc;
+  std::vector<double> r_max(s->n_scenes, 0.0);
+  for (int sc = 0; sc < s->n_scenes; ++sc)
+    for (int64_t i = s->pbase[sc]; i < s->pbase[sc + 1]; ++i) r_max[sc] = std::max(r_max[sc], host[8 * i + 6]);
+  void* saved = nullptr;
+  rc = save_state(s, saved);
+  if (rc != PS_OK) return rc;
+  cudaEvent_t ea, eb;
+  PS_CUDA(cudaEventCreate(&ea));
+  PS_CUDA(cudaEventCreate(&eb));
+  // one trial: warm-up (captures the graphs), restore, timed steps, restore
+  auto trial = [&](double& ms_per_step) -> int {
+    int r = load_state(s, saved);
+    if (r == PS_OK) r = ps_step(s, std::min(trial_steps, s->graph_block));
+    if (r == PS_OK) r = load_state(s, saved);
+    if (r != PS_OK) return r;
+    cudaEventRecord(ea, s->stream);
+    r = ps_step(s, trial_steps);
+    cudaEventRecord(eb, s->stream);
+    if (cudaEventSynchronize(eb) != cudaSuccess) return fail(PS_ERR_CUDA, "ps_autotune: timing failed");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ea, eb);
+    ms_per_step = (double)ms / (double)trial_steps;
+    if (r == PS_OK) r = check_device_error(s);
+    return r;
+  };
+  auto apply_factor = [&](double f) -> int {
+    for (int sc = 0; sc < s->n_scenes; ++sc)
+      if (r_max[sc] > 0.0) s->desc[sc].cell_size = f * 2.0 * r_max[sc];
+    return resize_grids(s, host);
+  };
+  double before = 0.0;
+  rc = trial(before);
+  double best = INFINITY, best_f = cell_factors[0];
+  int64_t best_l = graph_blocks[0];
+  for (int32_t f = 0; f < n_factors && rc == PS_OK; ++f) {
+    rc = apply_factor(cell_factors[f]);
+    for (int32_t l = 0; l < n_blocks && rc == PS_OK; ++l) {
+      for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+      s->graphs.clear();
+      s->graph_block = graph_blocks[l];
+      double ms = 0.0;
+      rc = trial(ms);
+      if (ms_table != nullptr) ms_table[(size_t)f * (size_t)n_blocks + (size_t)l] = ms;
+      if (rc == PS_OK && ms < best) {
+        best = ms;
+        best_f = cell_factors[f];
+        best_l = graph_blocks[l];
+      }
+    }
+  }
+  if (rc == PS_OK) rc = apply_factor(best_f);
+  for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+  s->graph_block = best_l;
+  if (rc == PS_OK) rc = load_state(s, saved);
+  if (rc == PS_OK) rc = ps_sync(s);
+  cudaEventDestroy(ea);
+  cudaEventDestroy(eb);
+  cudaFree(saved);
+  if (rc != PS_OK) return rc;
+  out->cell_factor = best_f;
+  out->graph_block = best_l;
+  out->ms_per_step = best;
+  out->before_ms_per_step = before;
+  return PS_OK;
 }
 
 extern "C" int ps_profile_steps(ps_sim* s, int64_t n_steps, double* kernel_ms, int64_t* kernel_launches) {

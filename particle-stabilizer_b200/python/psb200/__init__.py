@@ -27,7 +27,7 @@ EXPORTED = (
     "ps_grid_get", "ps_buckets_get", "ps_last_launch_count", "ps_destroy", "ps_simulate",
     "ps_exclusive_scan_scratch_bytes", "ps_exclusive_scan_u32", "ps_read_csv", "ps_write_csv", "ps_read_obj",
     "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "ps_forward_checkpointed",
-    "ps_backward", "ps_exclusive_scan_u32_noalloc", "runSimulateCUDA",
+    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_autotune", "runSimulateCUDA",
 )
 KERNEL_KINDS = ("begin", "scan", "scatter", "rank_move", "contacts")
 
@@ -56,6 +56,11 @@ class Grad(C.Structure):
     def as_array(self) -> np.ndarray:
         """(k_spring, e_sphere, e_wall[0..5]) in the reference's wall order."""
         return np.array([self.k_spring, self.e_sphere, *self.e_wall])
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("cell_factor", C.c_double), ("graph_block", C.c_int64), ("ms_per_step", C.c_double),
+                ("before_ms_per_step", C.c_double)]
 
 
 class PSError(RuntimeError):
@@ -98,6 +103,8 @@ def lib() -> C.CDLL:
         L.ps_forward_checkpointed.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
         L.ps_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ps_exclusive_scan_u32_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        L.ps_autotune.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                                  C.POINTER(TuneResult)]
         _lib = L
     return _lib
 
@@ -215,6 +222,22 @@ class Simulation:
     def forward_checkpointed(self, n_steps: int, every: int) -> None:
         """Advance n_steps keeping a checkpoint every `every` steps (for backward)."""
         _check(lib().ps_forward_checkpointed(self.h, int(n_steps), int(every)), "ps_forward_checkpointed")
+
+    def autotune(self, trial_steps: int = 20, cell_factors=(1.0, 1.05, 1.25, 1.5, 2.0),
+                 graph_blocks=(50, 100, 200)) -> dict:
+        """Time `trial_steps` steps from the current state for every cell-size
+        factor (cell edge = factor * 2 * r_max per scene) and graph block
+        length, keep the fastest pair and restore the state (ps_autotune)."""
+        f = np.ascontiguousarray(cell_factors, dtype=np.float64)
+        b = np.ascontiguousarray(graph_blocks, dtype=np.int64)
+        table = np.zeros((f.size, b.size), dtype=np.float64)
+        res = TuneResult()
+        _check(lib().ps_autotune(self.h, int(trial_steps), _ptr(f), int(f.size), _ptr(b), int(b.size), _ptr(table),
+                                 C.byref(res)), "ps_autotune")
+        return {"cell_factor": res.cell_factor, "graph_block": int(res.graph_block),
+                "ms_per_step": res.ms_per_step, "before_ms_per_step": res.before_ms_per_step,
+                "cell_factors": [float(x) for x in f], "graph_blocks": [int(x) for x in b],
+                "ms_table": table.tolist()}
 
     def backward(self, dl_dstate: np.ndarray):
         """Gradients of a loss of the final state: dl_dstate is (n, 6) =

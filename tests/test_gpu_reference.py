@@ -61,3 +61,44 @@ def test_counts_offsets_sets_equal_reference(need_gpu, make, steps):
     scale = np.abs(ref_state).max(axis=0) + 1e-300
     rel = (np.abs(st - ref_state) / scale).max()
     assert rel < 1e-12, rel
+
+
+@needs_ref
+def test_head_to_head_with_reference_cuda_at_1m_spheres(need_gpu):
+    """Throughput against the reference's own CUDA build on the same B200:
+    the 1,048,576-sphere scene with a spring the scheme integrates stably
+    (k = 0.25; with the specified 5e4 the scheme diverges and the reference
+    build indexes out of range once positions stop being finite).  Both run
+    steps 21..220 from the same initial state; the reference runs only after
+    this library's FP64 run of the same steps stayed finite and inside the
+    box.  Target: at least 3x the reference's particle-steps/s."""
+    import time
+
+    sc = scenes.c2_scene(k_spring=0.25)
+    warm, steps = 20, 200
+    ours = {}
+    for prec in ("f32", "f64"):
+        with psb200.Simulation(sc, prec) as sim:
+            sim.set_state()
+            sim.step(warm)
+            ms = sim.time_steps(steps)
+            st = sim.get_state()
+        ours[prec] = sc.n * steps / (ms * 1e-3)
+        assert np.isfinite(st).all()
+        assert np.all(st[:, :3] >= np.array(sc.box_min)) and np.all(st[:, :3] <= np.array(sc.box_max))
+    r = O.ref_cuda()
+    t0 = time.perf_counter()
+    h = r.create(sc)
+    try:
+        r.step(h, warm)
+        ref_s = r.time_steps(h, steps)
+        ref_state = r.state(h, sc.n)
+    finally:
+        r.destroy(h)
+    assert np.isfinite(ref_state).all()
+    ref = sc.n * steps / ref_s
+    print(f"\n1M spheres, steps {warm + 1}..{warm + steps}: reference CUDA (FP64) {ref:.3e} particle-steps/s "
+          f"({1e3 * ref_s / steps:.3f} ms/step); this library FP64 {ours['f64']:.3e} ({ours['f64'] / ref:.1f}x), "
+          f"FP32 {ours['f32']:.3e} ({ours['f32'] / ref:.1f}x); reference set-up and warm-up "
+          f"{time.perf_counter() - t0 - ref_s:.1f} s")
+    assert ours["f64"] >= 3.0 * ref and ours["f32"] >= 3.0 * ref
