@@ -44,6 +44,10 @@ UNIT = "particle-steps/s"
 WORKLOAD = ("1,048,576 spheres, log-normal r (median 0.002, sigma 0.25, clip [0.001,0.004]), box 1x1x4, "
             "k 5e4, e 0.4, walls 0.7, dt 5e-6, cell 2 r_max")
 L2_BYTES = 126 * 2 ** 20
+# DRAM bytes per launch of the fused FP32 contacts kernel on this workload,
+# measured with ncu in steady state (33.6 MB read + 54.4 MB written; the
+# algorithmic bytes are 75.5 MB).
+CONTACTS_TRAFFIC = 88.07e6
 
 
 def peaks():
@@ -411,7 +415,10 @@ def run_ours(args, world, rank, local, dist):
                    "l2": f"working set {state_bytes / 2**20:.0f} MiB > 126 MiB L2; no flush",
                    "parallelism": f"{world} independent replicas (one per GPU, no collective)"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": CONTACTS_TRAFFIC if (dom == "contacts" and args.precision == "f32") else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch of the fused "
+                                       "contacts kernel on this workload, steady state (--cache-control none)",
                      "alg_bytes_per_launch": alg_bytes(dom, n, cells)},
         "step_roofline": {"alg_bytes_per_step": step_alg_bytes(n, cells), "achieved_gbs": step_gbs,
                           "frac": step_gbs / peak},

@@ -7,7 +7,8 @@
 //   k_begin     x += v dt, v += g dt, box walls / triangles, cell hash,
 //               warp-aggregated count                    (first step of a call)
 //   scan        exclusive scan of the cell counts        (ps_scan.cuh)
-//   k_scatter   orig id -> tmp[offset[c] + slot]; clears count[c]
+//   k_scatter   slot = --count[c] (atomic; leaves the counts at zero),
+//               orig id -> tmp[offset[c] + slot]
 //   k_rank_move canonical in-cell rank (ascending orig id), float4 state move
 //   k_contacts  27-cell Jacobi contacts; FUSED also runs the next step's
 //               integrate + container + hash + count in its epilogue
@@ -117,21 +118,18 @@ __device__ __forceinline__ void walls(vec4_t<T>& P, vec4_t<T>& V, const ScenePar
 }
 
 // ---- warp-aggregated cell count --------------------------------------------
-// Lanes hashing to the same cell share one atomicAdd; each receives a
-// distinct slot in [count_before, count_before + peers).  The same pass
-// accumulates the per-tile totals of the count array (SCAN_TILE cells per
-// tile) that the step's scan uses in place of a look-back.
-__device__ __forceinline__ uint32_t count_slot(uint32_t* count, uint32_t* tile_sum, uint32_t c, bool valid) {
+// Lanes hashing to the same cell share one atomic add, whose result is not
+// used (a reduction: the warp does not wait for it); the slot inside the
+// cell is taken later by k_scatter.  The same pass accumulates the per-tile
+// totals of the count array (SCAN_TILE cells per tile) that the step's scan
+// uses in place of a look-back.
+__device__ __forceinline__ void count_cell(uint32_t* count, uint32_t* tile_sum, uint32_t c, bool valid) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned active = __ballot_sync(0xffffffffu, valid);
-  uint32_t slot = 0;
   if (valid) {
     const unsigned peers = __match_any_sync(active, c);
     const int leader = __ffs(peers) - 1;
-    uint32_t base = 0;
-    if ((int)lane == leader) base = atomicAdd(count + c, (uint32_t)__popc(peers));
-    base = __shfl_sync(peers, base, leader);
-    slot = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+    if ((int)lane == leader) atomicAdd(count + c, (uint32_t)__popc(peers));
     const uint32_t t = c / (uint32_t)SCAN_TILE;
     const int first = __ffs(active) - 1;
     if (__all_sync(active, t == __shfl_sync(active, t, first))) {
@@ -142,7 +140,6 @@ __device__ __forceinline__ uint32_t count_slot(uint32_t* count, uint32_t* tile_s
       if ((int)lane == __ffs(tpeers) - 1) atomicAdd(tile_sum + t, (uint32_t)__popc(tpeers));
     }
   }
-  return slot;
 }
 
 template <class T>
@@ -215,19 +212,19 @@ __global__ void __launch_bounds__(STEP_THREADS) k_begin(StepBufs<T> b, ScenePara
     b.V1[p] = V;
     b.cell[p] = c;
   }
-  const uint32_t s = count_slot(b.count, b.tile_sum, c, valid);
-  if (valid) b.slot[p] = s;
+  count_cell(b.count, b.tile_sum, c, valid);
 }
 
 constexpr int MOVE_PER_THREAD = 4;
 
-// tmp[offset[c] + slot] = orig; count[c] = 0 (every non-zero count belongs
-// to a cell some particle hashed to, so this restores an all-zero array) and
-// the tile totals are cleared for the next count.
+// slot = --count[c], a distinct slot of the cell for every member (the
+// decrements bring every count back to zero for the next step);
+// tmp[offset[c] + slot] = orig, and the slot is kept for k_rank_move.  The
+// tile totals are cleared for the next count.
 // MOVE_PER_THREAD particles per thread, strided by the block so that every
 // load instruction stays coalesced; all loads are issued before the stores.
 __global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __restrict__ cell,
-                                                          const uint32_t* __restrict__ slot,
+                                                          uint32_t* __restrict__ slot,
                                                           const uint32_t* __restrict__ orig,
                                                           const uint32_t* __restrict__ offset, uint32_t* tmp,
                                                           uint32_t* count, uint32_t n, uint32_t* tile_sum,
@@ -240,16 +237,19 @@ __global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __rest
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     const uint32_t p = base + k * STEP_THREADS;
     c[k] = p < n ? cell[p] : 0u;
-    sl[k] = p < n ? slot[p] : 0u;
     o[k] = p < n ? orig[p] : 0u;
   }
 #pragma unroll
-  for (int k = 0; k < MOVE_PER_THREAD; ++k) off[k] = (base + k * STEP_THREADS) < n ? __ldg(offset + c[k]) : 0u;
+  for (int k = 0; k < MOVE_PER_THREAD; ++k) {
+    const bool in = (base + k * STEP_THREADS) < n;
+    off[k] = in ? __ldg(offset + c[k]) : 0u;
+    sl[k] = in ? atomicSub(count + c[k], 1u) - 1u : 0u;
+  }
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     if (base + k * STEP_THREADS < n) {
       tmp[off[k] + sl[k]] = o[k];
-      count[c[k]] = 0u;
+      slot[base + k * STEP_THREADS] = sl[k];
     }
   }
 }
@@ -399,8 +399,7 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 5 : 4) k_contac
     }
   }
   if (FUSED) {
-    const uint32_t s = count_slot(b.count, b.tile_sum, c, valid);
-    if (valid) b.slot[i] = s;
+    count_cell(b.count, b.tile_sum, c, valid);
   }
 }
 

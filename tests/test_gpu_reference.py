@@ -102,3 +102,40 @@ def test_head_to_head_with_reference_cuda_at_1m_spheres(need_gpu):
           f"FP32 {ours['f32']:.3e} ({ours['f32'] / ref:.1f}x); reference set-up and warm-up "
           f"{time.perf_counter() - t0 - ref_s:.1f} s")
     assert ours["f64"] >= 3.0 * ref and ours["f32"] >= 3.0 * ref
+
+
+@needs_ref
+def test_head_to_head_on_the_4096_sphere_lattice(need_gpu):
+    """The reference's own CUDA build (5,000 steps) and CPU simulator (a
+    500-step sample, one thread) against this library on the 4,096-sphere
+    lattice, FP32 and FP64, all from the initial state.  The scene is small,
+    so both GPU paths are bound by per-step launch cost; target at least 3x
+    the reference CUDA build."""
+    sc = scenes.lattice_c1()
+    steps = 5000
+    ours = {}
+    for prec in ("f32", "f64"):
+        with psb200.Simulation(sc, prec) as sim:
+            sim.set_state()
+            sim.checkpoint_save(0)
+            sim.step(400)  # captures the step graphs
+            sim.checkpoint_load(0)
+            ms = sim.time_steps(steps)
+        ours[prec] = sc.n * steps / (ms * 1e-3)
+    r = O.ref_cuda()
+    h = r.create(sc)
+    try:
+        ref_cuda = sc.n * steps / r.time_steps(h, steps)
+    finally:
+        r.destroy(h)
+    c = O.ref_cpu()
+    h = c.create(sc)
+    try:
+        cpu_steps = 500
+        ref_cpu = sc.n * cpu_steps / c.time_steps(h, cpu_steps)
+    finally:
+        c.destroy(h)
+    print(f"\n4,096-sphere lattice: reference CUDA (FP64) {ref_cuda:.3e} particle-steps/s, reference CPU (1 thread, "
+          f"{cpu_steps}-step sample) {ref_cpu:.3e}; this library FP64 {ours['f64']:.3e} ({ours['f64'] / ref_cuda:.1f}x "
+          f"the reference CUDA), FP32 {ours['f32']:.3e} ({ours['f32'] / ref_cuda:.1f}x)")
+    assert ours["f64"] >= 3.0 * ref_cuda and ours["f32"] >= 3.0 * ref_cuda
