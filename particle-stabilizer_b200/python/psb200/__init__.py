@@ -164,8 +164,13 @@ class Simulation:
         st = np.ascontiguousarray(state, dtype=np.float64)
         _check(lib().ps_set_state(self.h, _ptr(st), st.shape[0]), "ps_set_state")
 
-    def get_state(self) -> np.ndarray:
-        out = np.empty((self.n, 8), dtype=np.float64)
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The state in original order, (n, 8) float64; `out` may be a
+        C-contiguous (n, 8) float64 buffer (for example in pinned memory)."""
+        if out is None:
+            out = np.empty((self.n, 8), dtype=np.float64)
+        if out.shape != (self.n, 8) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous (n, 8) float64 array")
         _check(lib().ps_get_state(self.h, _ptr(out), self.n), "ps_get_state")
         return out
 
