@@ -249,6 +249,25 @@ int ps_write_csv(const char* path, const double* aos, int64_t n);
  * vertices read in single precision as assimp's default ai_real. */
 int ps_read_obj(const char* path, double* tri_out, int64_t cap, int64_t* n_tri_out);
 
+/* ---- after the path: the CLI's post-processing of a result (host code) ----
+ * ps_resolve_overlaps   ParticleModel::resolveOverlaps
+ *                       (src/ParticleStabilizer/ParticleModel.cpp:154-259):
+ *   walks the particles in ascending order of coordinate `axis` (0, 1, 2) and
+ *   lifts each along that axis onto the first lower-ranked particle it
+ *   overlaps, re-ranking as the reference does; positions in `aos` (n x 8
+ *   reference records) are updated in place, with the reference's results.
+ *   If n_collided and max_overlap are not NULL they receive the closing
+ *   overlap check (as ps_overlap_stats).  Non-finite positions are rejected.
+ * ps_overlap_stats      the reference's closing check (ParticleModel.cpp:232-256):
+ *   particles overlapping a higher-indexed particle, and the largest
+ *   r_i + r_j - |x_i - x_j|; grid-based instead of O(N^2).
+ * ps_write_obj_spheres  ObjData::write (src/ParticleStabilizer/ObjData.cpp:8-140):
+ *   every particle as a triangulated sphere; the same text, formatted in
+ *   parallel. */
+int ps_resolve_overlaps(double* aos, int64_t n, int32_t axis, int64_t* n_collided, double* max_overlap);
+int ps_overlap_stats(const double* aos, int64_t n, int64_t* n_collided, double* max_overlap);
+int ps_write_obj_spheres(const char* path, const double* aos, int64_t n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -225,7 +225,22 @@ def ref_cpu() -> _RefLib:
     r.lib.refh_write_csv.argtypes = [C.c_void_p, C.c_int64, C.c_char_p]
     r.lib.refh_read_obj.restype = C.c_int64
     r.lib.refh_read_obj.argtypes = [C.c_char_p, C.c_void_p, C.c_int64]
+    r.lib.refh_resolve_overlaps.argtypes = [C.c_void_p, C.c_int64, C.c_int32]
+    r.lib.refh_write_obj.argtypes = [C.c_char_p, C.c_void_p, C.c_int64]
     return r
+
+
+def ref_resolve_overlaps(state: np.ndarray, axis: int) -> np.ndarray:
+    """The reference's own ParticleModel::resolveOverlaps on a copy of state."""
+    st = np.array(state, dtype=np.float64, order="C", copy=True)
+    ref_cpu().lib.refh_resolve_overlaps(_p(st), st.shape[0], int(axis))
+    return st
+
+
+def ref_write_obj(path: str, state: np.ndarray) -> None:
+    """The reference's own ObjData::write."""
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    ref_cpu().lib.refh_write_obj(path.encode(), _p(st), st.shape[0])
 
 
 def ref_cuda() -> _RefLib:

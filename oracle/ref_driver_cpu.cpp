@@ -5,8 +5,10 @@
 // PolygonContainer,ParticleIO}.cpp) into oracle/_ref/libref_cpu.so.  It
 // drives the per-step body of PhysicsEngine::startSimulationLoop
 // (src/ParticleStabilizer/PhysicsEngine.cpp:38-48) without the O(N^2)
-// statistics block, and exposes the reference's CSV reader/writer.
+// statistics block, and exposes the reference's CSV reader/writer and the
+// CLI's post-processing (ParticleModel::resolveOverlaps, ObjData::write).
 #include <ParticleStabilizer/BoxContainer.hpp>
+#include <ParticleStabilizer/ObjData.hpp>
 #include <ParticleStabilizer/ParticleIO.hpp>
 #include <ParticleStabilizer/ParticleModel.hpp>
 #include <ParticleStabilizer/PolygonContainer.hpp>
@@ -147,6 +149,35 @@ int64_t refh_read_obj(const char* path, double* tri_out, int64_t cap) {
     }
   }
   return n_tri;
+}
+
+namespace {
+std::vector<Particle> records_to_particles(const double* aos, int64_t n) {
+  std::vector<Particle> v;
+  v.reserve((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    const double* q = aos + 8 * i;
+    v.emplace_back(glm::dvec3(q[0], q[1], q[2]), glm::dvec3(q[3], q[4], q[5]), q[6], q[7]);
+  }
+  return v;
+}
+}  // namespace
+
+// ParticleModel::resolveOverlaps (ParticleModel.cpp:154-259); positions
+// written back into aos.
+void refh_resolve_overlaps(double* aos, int64_t n, int32_t axis) {
+  std::vector<Particle> v = records_to_particles(aos, n);
+  ParticleModel::resolveOverlaps(v, axis);
+  for (int64_t i = 0; i < n; ++i) {
+    aos[8 * i + 0] = v[(size_t)i].position.x;
+    aos[8 * i + 1] = v[(size_t)i].position.y;
+    aos[8 * i + 2] = v[(size_t)i].position.z;
+  }
+}
+
+// ObjData::write (ObjData.cpp:8-140).
+void refh_write_obj(const char* path, const double* aos, int64_t n) {
+  ObjData::write(std::string(path), records_to_particles(aos, n));
 }
 
 }  // extern "C"

@@ -7,8 +7,10 @@
 // reference's CPU simulator is not part of this build: the B200 path runs
 // whether or not --cuda is given.  Extra flags: --fp32 (single precision),
 // --cell-size S, --widen-domain, --lib PATH.  --visualize has no graphics
-// stack to open and --resolve-overlap-axis / --out-obj-path are the
-// post-processing steps after the path; all three are reported and skipped.
+// stack to open and is reported and skipped.  After the run, as the
+// reference (ParticleStabilizerMain.cpp:274-296): --resolve-overlap-axis
+// (ps_resolve_overlaps), then the CSV, then --out-obj-path
+// (ps_write_obj_spheres).
 #include <dlfcn.h>
 
 #include <cstdio>
@@ -27,6 +29,8 @@ using runSimulateCUDA_t = void (*)(const std::vector<ParticlePtr>&, const dvec3,
                                    const double, const size_t, const bool, std::vector<Particle>&);
 using read_csv_t = int (*)(const char*, const double*, double, double*, int64_t, int64_t*);
 using write_csv_t = int (*)(const char*, const double*, int64_t);
+using resolve_t = int (*)(double*, int64_t, int32_t, int64_t*, double*);
+using write_obj_t = int (*)(const char*, const double*, int64_t);
 using last_error_t = const char* (*)();
 
 namespace {
@@ -119,7 +123,9 @@ int main(int argc, char** argv) {
   auto read_csv = reinterpret_cast<read_csv_t>(dlsym(h, "ps_read_csv"));
   auto write_csv = reinterpret_cast<write_csv_t>(dlsym(h, "ps_write_csv"));
   auto last_error = reinterpret_cast<last_error_t>(dlsym(h, "ps_last_error"));
-  if (!run || !read_csv || !write_csv || !last_error) {
+  auto resolve = reinterpret_cast<resolve_t>(dlsym(h, "ps_resolve_overlaps"));
+  auto write_obj = reinterpret_cast<write_obj_t>(dlsym(h, "ps_write_obj_spheres"));
+  if (!run || !read_csv || !write_csv || !last_error || !resolve || !write_obj) {
     std::cerr << "Cannot load symbol: 'runSimulateCUDA' from the shared library.\n";
     return EXIT_FAILURE;
   }
@@ -146,21 +152,40 @@ int main(int argc, char** argv) {
   run(particles, a.boxMin, a.boxMax, a.containerPath, a.gravity, a.e_wall, a.k, a.e_sphere, a.dt, (size_t)a.maxSteps,
       a.toVisualize, result);
 
-  if (a.resolveOverlapAxis >= 0) std::cout << "[warning] --resolve-overlap-axis is not part of this build; skipped\n";
-  if (!a.objOutPath.empty()) std::cout << "[warning] --out-obj-path is not part of this build; skipped\n";
-  if (!a.particleOutPath.empty()) {
-    for (int64_t i = 0; i < n; ++i) {
-      double* q = aos.data() + 8 * i;
-      const Particle& p = result[(size_t)i];
-      q[0] = p.position.x; q[1] = p.position.y; q[2] = p.position.z;
-      q[3] = p.velocity.x; q[4] = p.velocity.y; q[5] = p.velocity.z;
-      q[6] = p.radius; q[7] = p.mass;
+  for (int64_t i = 0; i < n; ++i) {
+    double* q = aos.data() + 8 * i;
+    const Particle& p = result[(size_t)i];
+    q[0] = p.position.x; q[1] = p.position.y; q[2] = p.position.z;
+    q[3] = p.velocity.x; q[4] = p.velocity.y; q[5] = p.velocity.z;
+    q[6] = p.radius; q[7] = p.mass;
+  }
+  if (a.resolveOverlapAxis >= 0) {  // ParticleModel::resolveOverlaps (ParticleModel.cpp:154-259)
+    std::cout << "[info] ### Resolving overlaps\n";
+    int64_t n_collided = 0;
+    double max_overlap = 0.0;
+    if (resolve(aos.data(), n, a.resolveOverlapAxis, &n_collided, &max_overlap) != PS_OK) {
+      std::cerr << "[error] " << last_error() << "\n";
+      return EXIT_FAILURE;
     }
+    char line[128];
+    std::snprintf(line, sizeof(line), "Max collision distance: %.15lf", max_overlap);
+    std::cout << "[info] Number of collided particles: " << n_collided << " / " << n << "\n"
+              << "[info] " << line << "\n[info] ### Finished resolving overlaps\n";
+  }
+  if (!a.particleOutPath.empty()) {
     if (write_csv(a.particleOutPath.c_str(), aos.data(), n) != PS_OK) {
       std::cerr << "[error] " << last_error() << "\n";
       return EXIT_FAILURE;
     }
     std::cout << "[info] Finished writing to file " << a.particleOutPath << "\n";
+  }
+  if (!a.objOutPath.empty()) {  // ObjData::write (ObjData.cpp:8-140)
+    std::cout << "[info] Writing to file " << a.objOutPath << "\n";
+    if (write_obj(a.objOutPath.c_str(), aos.data(), n) != PS_OK) {
+      std::cerr << "[error] " << last_error() << "\n";
+      return EXIT_FAILURE;
+    }
+    std::cout << "[info] Finished writing to file " << a.objOutPath << "\n";
   }
   std::cout << "[info] Simulation completed successfully.\n";
   return EXIT_SUCCESS;

@@ -27,7 +27,8 @@ EXPORTED = (
     "ps_grid_get", "ps_buckets_get", "ps_last_launch_count", "ps_destroy", "ps_simulate",
     "ps_exclusive_scan_scratch_bytes", "ps_exclusive_scan_u32", "ps_read_csv", "ps_write_csv", "ps_read_obj",
     "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "ps_forward_checkpointed",
-    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_autotune", "runSimulateCUDA",
+    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_autotune", "ps_resolve_overlaps", "ps_overlap_stats",
+    "ps_write_obj_spheres", "runSimulateCUDA",
 )
 KERNEL_KINDS = ("begin", "scan", "scatter", "rank_move", "contacts")
 
@@ -103,6 +104,10 @@ def lib() -> C.CDLL:
         L.ps_forward_checkpointed.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
         L.ps_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ps_exclusive_scan_u32_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        L.ps_resolve_overlaps.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int64),
+                                          C.POINTER(C.c_double)]
+        L.ps_overlap_stats.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+        L.ps_write_obj_spheres.argtypes = [C.c_char_p, C.c_void_p, C.c_int64]
         L.ps_autotune.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
                                   C.POINTER(TuneResult)]
         _lib = L
@@ -335,3 +340,31 @@ def read_obj(path: str) -> np.ndarray:
     out = np.empty((n.value, 9), dtype=np.float64)
     _check(lib().ps_read_obj(path.encode(), _ptr(out), n.value, C.byref(n)), "ps_read_obj")
     return out
+
+
+# ---- after the path (host code in the library) --------------------------------
+def resolve_overlaps(state: np.ndarray, axis: int = 2):
+    """ParticleModel::resolveOverlaps on a copy of `state` (n x 8 records):
+    returns (new state, particles still overlapping a higher index, largest
+    remaining overlap)."""
+    st = np.array(state, dtype=np.float64, order="C", copy=True)
+    nc = C.c_int64()
+    mo = C.c_double()
+    _check(lib().ps_resolve_overlaps(_ptr(st), st.shape[0], int(axis), C.byref(nc), C.byref(mo)),
+           "ps_resolve_overlaps")
+    return st, int(nc.value), float(mo.value)
+
+
+def overlap_stats(state: np.ndarray):
+    """(particles overlapping a higher-indexed particle, largest overlap)."""
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    nc = C.c_int64()
+    mo = C.c_double()
+    _check(lib().ps_overlap_stats(_ptr(st), st.shape[0], C.byref(nc), C.byref(mo)), "ps_overlap_stats")
+    return int(nc.value), float(mo.value)
+
+
+def write_obj_spheres(path: str, state: np.ndarray) -> None:
+    """ObjData::write: every particle as a triangulated sphere."""
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    _check(lib().ps_write_obj_spheres(path.encode(), _ptr(st), st.shape[0]), "ps_write_obj_spheres")

@@ -80,3 +80,38 @@ def test_cli_runs_the_path_with_an_obj_container(need_gpu, tmp_path):
     ref_csv = tmp_path / "want.csv"
     psb200.write_csv(str(ref_csv), want)
     assert csv_out.read_text() == ref_csv.read_text()
+
+
+def test_cli_resolves_overlaps_and_writes_obj(need_gpu, tmp_path):
+    """--resolve-overlap-axis and --out-obj-path after the run, in the
+    reference's order: the CSV equals the oracle's FP64 state after the
+    reference's own resolveOverlaps (or this library's, which the CPU tests
+    show identical, when the reference build is absent)."""
+    sc = scenes.pile(400, seed=19, k_spring=1.0)
+    csv_in = tmp_path / "in.csv"
+    with open(csv_in, "w") as f:
+        f.write("x,y,z,r\n")
+        for p in sc.state:
+            f.write("%.17g,%.17g,%.17g,%.17g\n" % (p[0], p[1], p[2], p[6]))
+    csv_out, obj_out = tmp_path / "out.csv", tmp_path / "objdir" / "out.obj"
+    lo, hi = sc.box_min, sc.box_max
+    cmd = [psb200.CLI_PATH, "--lib", psb200.LIB_PATH, str(csv_in), "--cuda", "--max-steps", "30",
+           "--box-min", *map(str, lo), "--box-max", *map(str, hi), "--dt", "1e-05", "--coeff-of-spring", "1",
+           "--coeff-of-restitution-sphere", "0.5", "--coeff-of-restitution-wall", *["0.7"] * 6,
+           "--gravity", "0", "0", "-9.8", "--initial-velocity", "0", "0", "0", "--density", "1000",
+           "--resolve-overlap-axis", "2", "--out-csv-path", str(csv_out), "--out-obj-path", str(obj_out)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Number of collided particles" in r.stdout and "Max collision distance" in r.stdout
+    start = psb200.read_csv(str(csv_in), (0.0, 0.0, 0.0), 1000.0)
+    stepped = O.run(sc.copy(state=start, e_wall=(0.7,) * 6), 30, "f64")
+    if os.path.exists(O.REF_CPU_SO):
+        want = O.ref_resolve_overlaps(stepped, 2)
+    else:
+        want, _, _ = psb200.resolve_overlaps(stepped, 2)
+    ref_csv = tmp_path / "want.csv"
+    psb200.write_csv(str(ref_csv), want)
+    assert csv_out.read_text() == ref_csv.read_text()
+    with open(obj_out) as f:
+        assert f.readline() == "o Generated particles\n"
+    obj_out.unlink()
