@@ -30,12 +30,14 @@ STEPS = int(G["steps"])
 SLAB = tuple(float(x) for x in G["slab"])
 HIST_TOP = float(G["hist_top"])
 
-# Tolerances for runs that are not bit-identical to the oracle's FP64 run,
-# about five times the differences measured on a B200 (FP32: 2e-5, 0.012,
-# 4e-4; reference CUDA build: 5.4e-4, 0.015, 7e-5).
-PACKING_TOL = 0.003  # absolute, on a slab packing fraction of 0.613
+# Tolerances for runs that are not bit-identical to the oracle's FP64 run.
+# The reference CUDA build sums contacts with FP64 atomics in arbitrary
+# order, so its pile differs from run to run; the largest differences seen
+# on a B200 over five runs were 0.0020 (packing), 0.023 (histogram) and
+# 0.37 % (mean height); FP32 gave 2e-5, 0.012 and 0.04 %.
+PACKING_TOL = 0.005  # absolute, on a slab packing fraction of 0.613
 HIST_TV_TOL = 0.06   # total-variation distance between height histograms (24 bins)
-ZMEAN_TOL = 0.002    # relative, on the mean centre height
+ZMEAN_TOL = 0.01     # relative, on the mean centre height
 
 
 def summary(sc, state):
@@ -49,6 +51,8 @@ def check_statistics(sc, state):
     assert np.isfinite(state).all()
     assert abs(packing - float(G["packing"])) <= PACKING_TOL, (packing, float(G["packing"]))
     tv = 0.5 * float(np.abs(hist - G["hist"]).sum())
+    print(f"\npacking {packing:.6f} (oracle {float(G['packing']):.6f}), histogram distance {tv:.4f}, "
+          f"mean height {zmean:.6f} (oracle {float(G['zmean']):.6f})")
     assert tv <= HIST_TV_TOL, tv
     assert abs(zmean - float(G["zmean"])) <= ZMEAN_TOL * float(G["zmean"]), (zmean, float(G["zmean"]))
 
