@@ -63,6 +63,11 @@ __device__ __forceinline__ float4 ld4<float>(const float4* p) {
   return __ldg(p);
 }
 
+// Wait until the grid this kernel depends on has completed and its writes
+// are visible, when it was launched with programmatic stream serialization
+// (it may then start while that grid drains); a no-op for a normal launch.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ---- per-scene parameters (device copy) -----------------------------------
 // Scenes are concatenated: scene s owns particle slots [pbase, pbase+pcount)
 // and cells [cbase, cbase + nb.x*nb.y*nb.z) of the global arrays.  The

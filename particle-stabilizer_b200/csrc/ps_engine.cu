@@ -129,6 +129,23 @@ namespace {
 
 int64_t n_scan(const ps_sim* s) { return s->c_total + 1; }
 
+// Launch with programmatic stream serialization: the kernel may start while
+// its predecessor on the stream drains; it waits (griddepcontrol.wait, a
+// no-op for a normal launch) before reading anything the predecessor wrote.
+template <typename... KArgs, typename... Args>
+void pdl_launch(void (*k)(KArgs...), unsigned g, unsigned blk, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(g);
+  cfg.blockDim = dim3(blk);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <class T>
 StepBufs<T> bufs(ps_sim* s) {
   StepBufs<T> b;
@@ -188,17 +205,21 @@ int64_t enqueue_steps(ps_sim* s, int64_t steps) {
   const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
   cudaStream_t st = s->stream;
   int64_t launches = 0;
-  k_begin<T, MULTI, MESH, true><<<gb, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+  const MeshView* mv = s->d_mesh_view;
+  const int64_t nsc = n_scan(s);
+  const uint32_t nt = (uint32_t)s->n_total;
+  pdl_launch(k_begin<T, MULTI, MESH, true>, gb, STEP_THREADS, st, b, sp0, mv);
   ++launches;
   for (int64_t k = 0; k < steps; ++k) {
-    k_scan_with_tile_sums<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->tile_sum);
-    k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
-                                                                         s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
-    k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
+    pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, nsc,
+               (const uint32_t*)s->tile_sum);
+    pdl_launch(k_scatter, move_blocks(s->n_total, b.n_tiles), STEP_THREADS, st, (const uint32_t*)s->cell, s->slot,
+               (const uint32_t*)s->orig, (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles);
+    pdl_launch(k_rank_move<T>, move_blocks(s->n_total, 0), STEP_THREADS, st, b);
     if (k + 1 < steps)
-      k_contacts<T, MULTI, MESH, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+      pdl_launch(k_contacts<T, MULTI, MESH, true>, gp, STEP_THREADS, st, b, sp0, mv);
     else
-      k_contacts<T, MULTI, MESH, false><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+      pdl_launch(k_contacts<T, MULTI, MESH, false>, gp, STEP_THREADS, st, b, sp0, mv);
     launches += 4;
   }
   return launches;
@@ -846,18 +867,21 @@ int enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes, 
     b.tape_p = row.p;
     b.tape_v = row.v;
     b.tape_o = row.o;
-    k_scan_with_tile_sums<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->tile_sum);
-    k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
-                                                                         s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
-    k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
+    pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, n_scan(s),
+               (const uint32_t*)s->tile_sum);
+    pdl_launch(k_scatter, move_blocks(s->n_total, b.n_tiles), STEP_THREADS, st, (const uint32_t*)s->cell, s->slot,
+               (const uint32_t*)s->orig, (const uint32_t*)s->offset, s->tmp, s->count, (uint32_t)s->n_total,
+               s->tile_sum, b.n_tiles);
+    pdl_launch(k_rank_move<T>, move_blocks(s->n_total, 0), STEP_THREADS, st, b);
     b.tape_vpre = row.vpre;
     b.tape_cell = row.cell;
     PS_CUDA(cudaMemcpyAsync(offs + offs_stride * (size_t)k, s->offset, sizeof(uint32_t) * (size_t)n_scan(s),
                             cudaMemcpyDeviceToDevice, st));
+    const MeshView* mv = s->d_mesh_view;
     if (k + 1 < steps)
-      k_contacts<T, MULTI, false, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+      pdl_launch(k_contacts<T, MULTI, false, true>, gp, STEP_THREADS, st, b, sp0, mv);
     else
-      k_contacts<T, MULTI, false, false><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+      pdl_launch(k_contacts<T, MULTI, false, false>, gp, STEP_THREADS, st, b, sp0, mv);
   }
   return PS_OK;
 }

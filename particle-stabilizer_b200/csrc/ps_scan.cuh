@@ -183,6 +183,8 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_with_tile_sums(const uint
   __shared__ uint32_t s_pre[SCAN_THREADS / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t tile = blockIdx.x;
+  pdl_wait();
+
   const int64_t wbase = tile * SCAN_TILE + (int64_t)warp * (32 * SCAN_ITEMS);
 
   uint32_t pre = 0;

@@ -197,6 +197,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_begin(StepBufs<T> b, ScenePara
   const uint32_t p = blockIdx.x * STEP_THREADS + threadIdx.x;
   const bool valid = p < b.n;
   uint32_t c = 0;
+  pdl_wait();
   if (valid) {
     const SceneParams<T>& sp = scene_of<T, MULTI>(p, sp0, b.scenes, b.pbase, b.n_scenes);
     vec4_t<T> P = b.P0[p];
@@ -229,6 +230,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __rest
                                                           const uint32_t* __restrict__ offset, uint32_t* tmp,
                                                           uint32_t* count, uint32_t n, uint32_t* tile_sum,
                                                           uint32_t n_tiles) {
+  pdl_wait();
   const uint32_t t = blockIdx.x * STEP_THREADS + threadIdx.x;
   if (t < n_tiles) tile_sum[t] = 0u;
   const uint32_t base = blockIdx.x * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
@@ -258,6 +260,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __rest
 // moves the integrated state (P1, V1) there as (P0, V0) with its orig id.
 template <class T>
 __global__ void __launch_bounds__(STEP_THREADS) k_rank_move(StepBufs<T> b) {
+  pdl_wait();
   const uint32_t base = blockIdx.x * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
   uint32_t c[MOVE_PER_THREAD], sl[MOVE_PER_THREAD];
 #pragma unroll
@@ -336,6 +339,7 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 5 : 4) k_contac
   const uint32_t i = blockIdx.x * STEP_THREADS + threadIdx.x;
   const bool valid = i < b.n;
   uint32_t c = 0;
+  pdl_wait();
   if (valid) {
     const SceneParams<T>& sp = scene_of<T, MULTI>(i, sp0, b.scenes, b.pbase, b.n_scenes);
     vec4_t<T> P = b.P0[i];
