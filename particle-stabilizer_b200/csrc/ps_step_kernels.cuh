@@ -117,19 +117,18 @@ __device__ __forceinline__ void walls(vec4_t<T>& P, vec4_t<T>& V, const ScenePar
   if (mxz > sp.box_hi[2]) { P.z = A::sub(sp.box_hi[2], r); V.z = A::mul(-V.z, sp.e_hi[2]); }
 }
 
-// ---- warp-aggregated cell count --------------------------------------------
-// Lanes hashing to the same cell share one atomic add, whose result is not
-// used (a reduction: the warp does not wait for it); the slot inside the
-// cell is taken later by k_scatter.  The same pass accumulates the per-tile
-// totals of the count array (SCAN_TILE cells per tile) that the step's scan
-// uses in place of a look-back.
+// ---- cell count ---------------------------------------------------------------
+// One atomic reduction per particle, whose result is not used (the warp
+// does not wait for it; at a few particles per cell lanes rarely share a
+// cell, so aggregating them first costs more than it saves); the slot
+// inside the cell is taken later by k_scatter.  The same pass accumulates,
+// warp-aggregated, the per-tile totals of the count array (SCAN_TILE cells
+// per tile) that the step's scan uses in place of a look-back.
 __device__ __forceinline__ void count_cell(uint32_t* count, uint32_t* tile_sum, uint32_t c, bool valid) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned active = __ballot_sync(0xffffffffu, valid);
   if (valid) {
-    const unsigned peers = __match_any_sync(active, c);
-    const int leader = __ffs(peers) - 1;
-    if ((int)lane == leader) atomicAdd(count + c, (uint32_t)__popc(peers));
+    atomicAdd(count + c, 1u);
     const uint32_t t = c / (uint32_t)SCAN_TILE;
     const int first = __ffs(active) - 1;
     if (__all_sync(active, t == __shfl_sync(active, t, first))) {
@@ -335,7 +334,7 @@ __device__ __forceinline__ void cell_coords(uint32_t c, const SceneParams<T>& sp
 }
 
 template <class T, bool MULTI, bool MESH, bool FUSED>
-__global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 5 : 4) k_contacts(StepBufs<T> b, SceneParams<T> sp0, const MeshView* mv) {
+__global__ void __launch_bounds__(STEP_THREADS, 4) k_contacts(StepBufs<T> b, SceneParams<T> sp0, const MeshView* mv) {
   const uint32_t i = blockIdx.x * STEP_THREADS + threadIdx.x;
   const bool valid = i < b.n;
   uint32_t c = 0;
