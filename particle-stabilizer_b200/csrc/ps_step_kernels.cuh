@@ -334,7 +334,8 @@ __device__ __forceinline__ void cell_coords(uint32_t c, const SceneParams<T>& sp
 }
 
 template <class T, bool MULTI, bool MESH, bool FUSED>
-__global__ void __launch_bounds__(STEP_THREADS, 4) k_contacts(StepBufs<T> b, SceneParams<T> sp0, const MeshView* mv) {
+__global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 4 : 3) k_contacts(StepBufs<T> b, SceneParams<T> sp0,
+                                                                                  const MeshView* mv) {
   const uint32_t i = blockIdx.x * STEP_THREADS + threadIdx.x;
   const bool valid = i < b.n;
   uint32_t c = 0;
