@@ -196,6 +196,25 @@ int ps_backward(ps_sim* sim, const double* dl_dstate, ps_grad* grads, double* dl
  * and equal to the oracle's with that cell size, but not bit-equal to runs
  * with the previous grid.  A recorded ps_forward_checkpointed is dropped.
  * Allocates device memory (grids, graphs, one state copy). */
+/* ---- neighbour-list mode (no counterpart in the reference, which rebuilds
+ * its grid every step, ParticleModelCUDA.cpp:115-155) ----
+ * ps_set_neighbor_lists(sim, skin_fraction, max_neighbours): with
+ * skin_fraction in [0.01, 1], ps_step keeps per-sphere lists of the spheres
+ * within r_i + r_j + skin (skin = skin_fraction x the scene's cell edge) and
+ * rebuilds grid and lists only when some sphere has moved about skin / 2
+ * since the last build (the device decides, step by step, through
+ * conditional graph nodes); 0 switches the mode off (the default).
+ * Results are bit-identical to the grid path: the overlapping pairs of each
+ * sphere are applied in the grid walk's order.  A list longer than
+ * max_neighbours, or more than 32 overlapping pairs on one sphere whose
+ * order changed since the build, makes ps_step repeat the whole call on the
+ * grid path from its starting state.  In this mode ps_step returns after the
+ * device has finished.
+ * ps_list_stats: rebuilds requested by the device and calls repeated on the
+ * grid path, both counted from the last ps_set_neighbor_lists. */
+int ps_set_neighbor_lists(ps_sim* sim, double skin_fraction, int32_t max_neighbours);
+int ps_list_stats(ps_sim* sim, int64_t* rebuilds, int64_t* fallbacks);
+
 typedef struct ps_tune_result {
   double cell_factor;        /* chosen f                                          */
   int64_t graph_block;       /* chosen L                                          */

@@ -63,6 +63,42 @@ __device__ __forceinline__ float4 ld4<float>(const float4* p) {
   return __ldg(p);
 }
 
+// Loads of data that the same kernel may have written earlier in its run (a
+// persistent kernel with grid barriers, COH = true) go through L2
+// (ld.global.cg); otherwise through the read-only path (ld_ro) or a plain
+// load (ld_pl), as the kernels launched once per phase use them.
+template <bool COH>
+__device__ __forceinline__ uint32_t ld_ro(const uint32_t* p) {
+  if constexpr (COH)
+    return __ldcg(p);
+  else
+    return __ldg(p);
+}
+template <bool COH>
+__device__ __forceinline__ uint32_t ld_pl(const uint32_t* p) {
+  if constexpr (COH)
+    return __ldcg(p);
+  else
+    return *p;
+}
+template <class T, bool COH>
+__device__ __forceinline__ vec4_t<T> ld4c(const vec4_t<T>* p) {
+  if constexpr (!COH) {
+    return ld4<T>(p);
+  } else if constexpr (sizeof(T) == 4) {
+    return __ldcg(p);
+  } else {
+    const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    vec4_t<T> v;
+    v.x = a.x;
+    v.y = a.y;
+    v.z = b.x;
+    v.w = b.y;
+    return v;
+  }
+}
+
 // Wait until the grid this kernel depends on has completed and its writes
 // are visible, when it was launched with programmatic stream serialization
 // (it may then start while that grid drains); a no-op for a normal launch.
@@ -132,6 +168,8 @@ enum : uint32_t {
   PS_DEVERR_SCAN_TIMEOUT = 1u << 0,   // decoupled look-back gave up waiting
   PS_DEVERR_MESH_OVERFLOW = 1u << 1,  // a particle hit more triangles than the hit buffer holds
   PS_DEVERR_BAD_CELL = 1u << 2,       // a cell id fell outside its scene (never expected)
+  PS_DEVERR_LIST_OVERFLOW = 1u << 3,  // neighbour-list mode: a list or a sphere's overlap buffer was full
+  PS_DEVERR_LIST_BARRIER = 1u << 4,   // neighbour-list mode: a grid barrier of the rebuild gave up waiting
 };
 
 }  // namespace psb

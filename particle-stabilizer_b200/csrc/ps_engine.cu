@@ -21,6 +21,7 @@
 
 #include "particle_stabilizer_b200.h"
 #include "ps_adjoint.cuh"
+#include "ps_lists.cuh"
 #include "ps_scan.cuh"
 #include "ps_stats.cuh"
 #include "ps_step_kernels.cuh"
@@ -122,6 +123,15 @@ struct ps_sim {
   std::vector<void*> fwd_ckpt;            // state at the start of each block, + final state last
   void* adj_arena = nullptr;              // tape, adjoint arrays, partials
   size_t adj_bytes = 0;
+  // neighbour-list mode (ps_set_neighbor_lists); off when list_skin <= 0
+  double list_skin = 0.0;                 // skin as a fraction of the cell edge
+  int32_t list_cap = 0;                   // list capacity per sphere
+  void* list_arena = nullptr;
+  size_t list_bytes = 0;
+  void* list_ckpt = nullptr;              // state at the start of a list-mode call
+  int64_t list_fallbacks = 0;             // calls repeated on the grid path after an overflow
+  int64_t list_rebuilds = 0;              // grid + list rebuilds requested by the device
+  unsigned list_rebuild_grid = 0;         // CTAs of the cooperative rebuild (one wave)
 };
 
 namespace {
@@ -281,6 +291,107 @@ void enqueue_steps_recorded_dispatch(ps_sim* s, int64_t steps, std::vector<Launc
     else
       enqueue_steps_recorded<T, false, false>(s, steps, rec);
   }
+}
+
+// ---- neighbour-list mode ---------------------------------------------------------
+size_t list_arena_bytes(const ps_sim* s) {
+  const size_t n = (size_t)std::max<int64_t>(s->n_total, 1), vb = s->precision == PS_FP32 ? 16 : 32;
+  return 5 * align_up(vb * n, 256) + 3 * align_up(4 * n, 256) + align_up(4 * n * (size_t)s->list_cap, 256) +
+         align_up(4 * LIST_FLAG_WORDS, 256);
+}
+
+template <class T>
+ListBufs<T> list_bufs(ps_sim* s) {
+  const size_t n = (size_t)std::max<int64_t>(s->n_total, 1);
+  const size_t b4 = align_up(sizeof(vec4_t<T>) * n, 256), bu = align_up(4 * n, 256);
+  char* p = static_cast<char*>(s->list_arena);
+  ListBufs<T> L;
+  L.P[0] = reinterpret_cast<vec4_t<T>*>(p); p += b4;
+  L.P[1] = reinterpret_cast<vec4_t<T>*>(p); p += b4;
+  L.V[0] = reinterpret_cast<vec4_t<T>*>(p); p += b4;
+  L.V[1] = reinterpret_cast<vec4_t<T>*>(p); p += b4;
+  L.ref = reinterpret_cast<vec4_t<T>*>(p); p += b4;
+  L.cell[0] = reinterpret_cast<uint32_t*>(p); p += bu;
+  L.cell[1] = reinterpret_cast<uint32_t*>(p); p += bu;
+  L.cnt = reinterpret_cast<uint32_t*>(p); p += bu;
+  L.list = reinterpret_cast<uint32_t*>(p); p += align_up(4 * n * (size_t)s->list_cap, 256);
+  L.flag = reinterpret_cast<uint32_t*>(p);
+  L.cap = (uint32_t)s->list_cap;
+  L.skin_frac = (T)s->list_skin;
+  return L;
+}
+
+// `steps` steps on neighbour lists: a full rebuild from the at-rest state,
+// then per step the gated cooperative rebuild and the list step kernel.
+// Every graph starts from zeroed counts, whatever an earlier rebuild left.
+template <class T, bool MULTI, bool MESH>
+cudaError_t enqueue_steps_list(ps_sim* s, int64_t steps) {
+  const StepBufs<T> b = bufs<T>(s);
+  const ListBufs<T> L = list_bufs<T>(s);
+  const SceneParams<T> sp0 = params<T>(s)[0];
+  const unsigned gp = blocks_for(s->n_total);
+  const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
+  const unsigned gm0 = move_blocks(s->n_total, b.n_tiles), gm1 = move_blocks(s->n_total, 0);
+  cudaStream_t st = s->stream;
+  const MeshView* mv = s->d_mesh_view;
+  const int64_t nsc = n_scan(s);
+  const uint32_t nt = (uint32_t)s->n_total;
+  cudaMemsetAsync(L.flag, 0, LIST_RESET_WORDS * sizeof(uint32_t), st);
+  cudaMemsetAsync(s->count, 0, sizeof(uint32_t) * (size_t)nsc, st);
+  cudaMemsetAsync(s->tile_sum, 0, sizeof(uint32_t) * (size_t)b.n_tiles, st);
+  pdl_launch(k_begin<T, MULTI, MESH, true>, gp, STEP_THREADS, st, b, sp0, mv);
+  pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, nsc,
+             (const uint32_t*)s->tile_sum);
+  pdl_launch(k_scatter, gm0, STEP_THREADS, st, (const uint32_t*)s->cell, s->slot, (const uint32_t*)s->orig,
+             (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles);
+  pdl_launch(k_rank_move<T>, gm1, STEP_THREADS, st, b);
+  pdl_launch(k_list_build<T, MULTI>, gp, STEP_THREADS, st, b, sp0, L, 0);
+  for (int64_t k = 0; k < steps; ++k) {
+    const int par = (int)(k & 1);
+    if (k > 0) {
+      // the rebuild works on state buffer `par`, in the order of the previous build
+      StepBufs<T> br = b;
+      br.P1 = L.P[par];
+      br.V1 = L.V[par];
+      br.cell = L.cell[par];
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(s->list_rebuild_grid);
+      cfg.blockDim = dim3(STEP_THREADS);
+      cfg.stream = st;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeCooperative;
+      at[0].val.cooperative = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      const cudaError_t e = cudaLaunchKernelEx(&cfg, k_list_rebuild<T, MULTI>, br, sp0, L, par, nsc, (uint32_t)gs,
+                                               (uint32_t)gm0, (uint32_t)gm1);
+      if (e != cudaSuccess) return e;
+    }
+    if (k + 1 < steps)
+      pdl_launch(k_contacts_list<T, MULTI, MESH, true>, gp, STEP_THREADS, st, b, sp0, mv, L, par);
+    else
+      pdl_launch(k_contacts_list<T, MULTI, MESH, false>, gp, STEP_THREADS, st, b, sp0, mv, L, par);
+  }
+  return cudaGetLastError();
+}
+
+// CTAs of one wave of k_list_rebuild, which its grid barriers need resident.
+template <class T, bool MULTI>
+int rebuild_grid(ps_sim* s, unsigned& grid) {
+  int per_sm = 0, sms = 0;
+  PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_list_rebuild<T, MULTI>, STEP_THREADS, 0));
+  PS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+  if (per_sm < 1 || sms < 1) return fail(PS_ERR_CUDA, "ps_step: the list rebuild kernel cannot be resident");
+  grid = (unsigned)(per_sm * sms);
+  return PS_OK;
+}
+
+template <class T>
+cudaError_t enqueue_steps_list_dispatch(ps_sim* s, int64_t steps) {
+  if (s->multi) {
+    return s->has_mesh ? enqueue_steps_list<T, true, true>(s, steps) : enqueue_steps_list<T, true, false>(s, steps);
+  }
+  return s->has_mesh ? enqueue_steps_list<T, false, true>(s, steps) : enqueue_steps_list<T, false, false>(s, steps);
 }
 
 template <class T>
@@ -760,6 +871,8 @@ void free_sim(ps_sim* s) {
   for (void* p : s->fwd_ckpt) cudaFree(p);
   s->fwd_ckpt.clear();
   cudaFree(s->adj_arena);
+  cudaFree(s->list_arena);
+  cudaFree(s->list_ckpt);
   if (s->l2_window_on) {
     cudaStreamAttrValue v{};
     v.accessPolicyWindow.num_bytes = 0;
@@ -1102,22 +1215,25 @@ extern "C" int ps_get_state(ps_sim* s, double* out, int64_t n_total) {
   return check_device_error(s);
 }
 
-extern "C" int ps_step(ps_sim* s, int64_t n_steps) {
-  if (s == nullptr || n_steps < 0) return fail(PS_ERR_INVALID, "ps_step: bad argument");
-  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_step: call ps_set_state first");
-  s->last_launches = 0;
-  if (n_steps == 0 || s->n_total == 0) return PS_OK;
-  DeviceGuard guard(s->device);
+namespace {
+
+// Run n_steps as CUDA graphs of up to graph_block steps (grid path, or the
+// neighbour-list path when `lists`), asynchronously.
+int step_graphs(ps_sim* s, int64_t n_steps, bool lists) {
   int64_t left = n_steps;
   while (left > 0) {
     const int64_t L = std::min(left, s->graph_block);
-    auto it = s->graphs.find(L);
+    const int64_t key = lists ? (L | (int64_t(1) << 62)) : L;
+    auto it = s->graphs.find(key);
     if (it == s->graphs.end()) {
       cudaGraph_t graph = nullptr;
       PS_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-      const int64_t nl = s->precision == PS_FP32 ? enqueue_steps_dispatch<float>(s, L) : enqueue_steps_dispatch<double>(s, L);
-      (void)nl;
-      const cudaError_t ce = cudaGetLastError();
+      cudaError_t ce = cudaSuccess;
+      if (lists)
+        ce = s->precision == PS_FP32 ? enqueue_steps_list_dispatch<float>(s, L) : enqueue_steps_list_dispatch<double>(s, L);
+      else
+        s->precision == PS_FP32 ? enqueue_steps_dispatch<float>(s, L) : enqueue_steps_dispatch<double>(s, L);
+      if (ce == cudaSuccess) ce = cudaGetLastError();
       const cudaError_t ee = cudaStreamEndCapture(s->stream, &graph);
       if (ce != cudaSuccess || ee != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -1128,13 +1244,114 @@ extern "C" int ps_step(ps_sim* s, int64_t n_steps) {
       const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
       cudaGraphDestroy(graph);
       if (ie != cudaSuccess) return fail(PS_ERR_CUDA, std::string("ps_step: instantiate failed: ") + cudaGetErrorString(ie));
-      it = s->graphs.emplace(L, exec).first;
+      it = s->graphs.emplace(key, exec).first;
     }
     PS_CUDA(cudaGraphLaunch(it->second, s->stream));
-    s->last_launches += 1 + 4 * L;
+    s->last_launches += lists ? 5 + 2 * L - 1 : 1 + 4 * L;
     left -= L;
   }
-  s->grid_valid = true;
+  return PS_OK;
+}
+
+// Neighbour-list path: exact as long as no list or overlap buffer overflows
+// (checked after the call); otherwise the call is repeated on the grid path
+// from the state it started from.
+int step_lists(ps_sim* s, int64_t n_steps) {
+  const size_t need = list_arena_bytes(s);
+  if (s->list_arena == nullptr || s->list_bytes < need) {
+    cudaFree(s->list_arena);
+    s->list_arena = nullptr;
+    s->list_bytes = 0;
+    for (auto it = s->graphs.begin(); it != s->graphs.end();) {  // list graphs hold the old buffers
+      if (it->first & (int64_t(1) << 62)) {
+        cudaGraphExecDestroy(it->second);
+        it = s->graphs.erase(it);
+      } else {
+        ++it;
+      }
+    }
+    PS_CUDA(cudaMalloc(&s->list_arena, need));
+    s->list_bytes = need;
+  }
+  if (s->list_rebuild_grid == 0) {
+    const int g = s->precision == PS_FP32
+                      ? (s->multi ? rebuild_grid<float, true>(s, s->list_rebuild_grid)
+                                  : rebuild_grid<float, false>(s, s->list_rebuild_grid))
+                      : (s->multi ? rebuild_grid<double, true>(s, s->list_rebuild_grid)
+                                  : rebuild_grid<double, false>(s, s->list_rebuild_grid));
+    if (g != PS_OK) return g;
+  }
+  uint32_t* rebuilds = s->precision == PS_FP32 ? list_bufs<float>(s).flag + LIST_REBUILDS
+                                               : list_bufs<double>(s).flag + LIST_REBUILDS;
+  PS_CUDA(cudaMemsetAsync(rebuilds, 0, sizeof(uint32_t), s->stream));
+  int rc = save_state(s, s->list_ckpt);
+  if (rc == PS_OK) rc = step_graphs(s, n_steps, true);
+  if (rc != PS_OK) return rc;
+  uint32_t e = 0, nr = 0;
+  PS_CUDA(cudaMemcpyAsync(&e, s->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+  PS_CUDA(cudaMemcpyAsync(&nr, rebuilds, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+  PS_CUDA(cudaStreamSynchronize(s->stream));
+  s->list_rebuilds += nr;
+  constexpr uint32_t list_err = PS_DEVERR_LIST_OVERFLOW | PS_DEVERR_LIST_BARRIER;
+  if (e & list_err) {
+    // counts and tile totals may be left over from an interrupted rebuild
+    const uint32_t rest = e & ~list_err;
+    PS_CUDA(cudaMemcpyAsync(s->err, &rest, sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+    PS_CUDA(cudaMemsetAsync(s->count, 0, sizeof(uint32_t) * (size_t)n_scan(s), s->stream));
+    PS_CUDA(cudaMemsetAsync(s->tile_sum, 0, sizeof(uint32_t) * (size_t)scan_num_tiles(n_scan(s)), s->stream));
+    PS_CUDA(cudaStreamSynchronize(s->stream));
+    ++s->list_fallbacks;
+    rc = load_state(s, s->list_ckpt);
+    if (rc == PS_OK) rc = step_graphs(s, n_steps, false);
+  }
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int ps_set_neighbor_lists(ps_sim* s, double skin_fraction, int32_t max_neighbours) {
+  if (s == nullptr || !(skin_fraction == 0.0 || (skin_fraction >= 0.01 && skin_fraction <= 1.0)) ||
+      (skin_fraction > 0.0 && (max_neighbours < 1 || max_neighbours > 4096)))
+    return fail(PS_ERR_INVALID,
+                "ps_set_neighbor_lists: skin_fraction must be 0 or in [0.01, 1], and max_neighbours in [1, 4096]");
+  DeviceGuard guard(s->device);
+  if (max_neighbours != s->list_cap) {  // the arena and the list graphs are rebuilt on the next step
+    cudaFree(s->list_arena);
+    s->list_arena = nullptr;
+    s->list_bytes = 0;
+  }
+  for (auto it = s->graphs.begin(); it != s->graphs.end();) {
+    if (it->first & (int64_t(1) << 62)) {
+      cudaGraphExecDestroy(it->second);
+      it = s->graphs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  s->list_skin = skin_fraction;
+  s->list_cap = skin_fraction > 0.0 ? max_neighbours : 0;
+  s->list_rebuilds = 0;
+  s->list_fallbacks = 0;
+  return PS_OK;
+}
+
+extern "C" int ps_list_stats(ps_sim* s, int64_t* rebuilds, int64_t* fallbacks) {
+  if (s == nullptr) return fail(PS_ERR_INVALID, "ps_list_stats: null simulation");
+  if (rebuilds != nullptr) *rebuilds = s->list_rebuilds;
+  if (fallbacks != nullptr) *fallbacks = s->list_fallbacks;
+  return PS_OK;
+}
+
+extern "C" int ps_step(ps_sim* s, int64_t n_steps) {
+  if (s == nullptr || n_steps < 0) return fail(PS_ERR_INVALID, "ps_step: bad argument");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_step: call ps_set_state first");
+  s->last_launches = 0;
+  if (n_steps == 0 || s->n_total == 0) return PS_OK;
+  DeviceGuard guard(s->device);
+  const bool lists = s->list_skin > 0.0;
+  const int rc = lists ? step_lists(s, n_steps) : step_graphs(s, n_steps, false);
+  if (rc != PS_OK) return rc;
+  s->grid_valid = !lists;  // after the list path the grid arrays do not describe the at-rest state
   s->stepped = true;
   return PS_OK;
 }

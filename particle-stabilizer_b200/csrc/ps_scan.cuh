@@ -175,20 +175,21 @@ __global__ void __launch_bounds__(SCAN_THREADS, 8) k_exclusive_scan_u32(const ui
 // holds elements 4*(32k + l) .. +3, so every load and store instruction of a
 // warp covers 512 contiguous bytes.  Rows are scanned with warp shuffles and
 // carried from row to row; warps are combined through shared memory.
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_with_tile_sums(const uint32_t* __restrict__ in,
-                                                                     uint32_t* __restrict__ out, int64_t n,
-                                                                     const uint32_t* __restrict__ tile_sum) {
+// One CTA scans tile `tile`; a CTA that scans several tiles in turn
+// synchronises its threads between them.
+template <bool COH>
+__device__ __forceinline__ void scan_tile_with_sums(int64_t tile, const uint32_t* __restrict__ in,
+                                                    uint32_t* __restrict__ out, int64_t n,
+                                                    const uint32_t* __restrict__ tile_sum) {
   constexpr int ROWS = SCAN_ITEMS / 4;  // uint4 per lane
   __shared__ uint32_t s_warp[SCAN_THREADS / 32];
   __shared__ uint32_t s_pre[SCAN_THREADS / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t tile = blockIdx.x;
-  pdl_wait();
 
   const int64_t wbase = tile * SCAN_TILE + (int64_t)warp * (32 * SCAN_ITEMS);
 
   uint32_t pre = 0;
-  for (int64_t t = tid; t < tile; t += SCAN_THREADS) pre += __ldg(tile_sum + t);
+  for (int64_t t = tid; t < tile; t += SCAN_THREADS) pre += ld_ro<COH>(tile_sum + t);
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) pre += __shfl_xor_sync(0xffffffffu, pre, d);
   if (lane == 0) s_pre[warp] = pre;
@@ -201,10 +202,10 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_with_tile_sums(const uint
     if (full) {
       v[k] = __ldcs(reinterpret_cast<const uint4*>(in + e));
     } else {
-      v[k].x = e + 0 < n ? in[e + 0] : 0u;
-      v[k].y = e + 1 < n ? in[e + 1] : 0u;
-      v[k].z = e + 2 < n ? in[e + 2] : 0u;
-      v[k].w = e + 3 < n ? in[e + 3] : 0u;
+      v[k].x = e + 0 < n ? ld_pl<COH>(in + e + 0) : 0u;
+      v[k].y = e + 1 < n ? ld_pl<COH>(in + e + 1) : 0u;
+      v[k].z = e + 2 < n ? ld_pl<COH>(in + e + 2) : 0u;
+      v[k].w = e + 3 < n ? ld_pl<COH>(in + e + 3) : 0u;
     }
   }
   // scan row by row inside the warp; `carry` is the warp's running total
@@ -244,6 +245,13 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_with_tile_sums(const uint
       if (e + 3 < n) out[e + 3] = y.w;
     }
   }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_with_tile_sums(const uint32_t* __restrict__ in,
+                                                                     uint32_t* __restrict__ out, int64_t n,
+                                                                     const uint32_t* __restrict__ tile_sum) {
+  pdl_wait();
+  scan_tile_with_sums<false>(blockIdx.x, in, out, n, tile_sum);
 }
 
 }  // namespace psb

@@ -223,27 +223,26 @@ constexpr int MOVE_PER_THREAD = 4;
 // tile totals are cleared for the next count.
 // MOVE_PER_THREAD particles per thread, strided by the block so that every
 // load instruction stays coalesced; all loads are issued before the stores.
-__global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __restrict__ cell,
-                                                          uint32_t* __restrict__ slot,
-                                                          const uint32_t* __restrict__ orig,
-                                                          const uint32_t* __restrict__ offset, uint32_t* tmp,
-                                                          uint32_t* count, uint32_t n, uint32_t* tile_sum,
-                                                          uint32_t n_tiles) {
-  pdl_wait();
-  const uint32_t t = blockIdx.x * STEP_THREADS + threadIdx.x;
+// Block `blk` of the scatter (COH: see ld_ro).
+template <bool COH>
+__device__ __forceinline__ void scatter_block(uint32_t blk, const uint32_t* __restrict__ cell,
+                                              uint32_t* __restrict__ slot, const uint32_t* __restrict__ orig,
+                                              const uint32_t* __restrict__ offset, uint32_t* tmp, uint32_t* count,
+                                              uint32_t n, uint32_t* tile_sum, uint32_t n_tiles) {
+  const uint32_t t = blk * STEP_THREADS + threadIdx.x;
   if (t < n_tiles) tile_sum[t] = 0u;
-  const uint32_t base = blockIdx.x * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
+  const uint32_t base = blk * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
   uint32_t c[MOVE_PER_THREAD], sl[MOVE_PER_THREAD], o[MOVE_PER_THREAD], off[MOVE_PER_THREAD];
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     const uint32_t p = base + k * STEP_THREADS;
-    c[k] = p < n ? cell[p] : 0u;
-    o[k] = p < n ? orig[p] : 0u;
+    c[k] = p < n ? ld_pl<COH>(cell + p) : 0u;
+    o[k] = p < n ? ld_pl<COH>(orig + p) : 0u;
   }
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     const bool in = (base + k * STEP_THREADS) < n;
-    off[k] = in ? __ldg(offset + c[k]) : 0u;
+    off[k] = in ? ld_ro<COH>(offset + c[k]) : 0u;
     sl[k] = in ? atomicSub(count + c[k], 1u) - 1u : 0u;
   }
 #pragma unroll
@@ -255,12 +254,21 @@ __global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __rest
   }
 }
 
+__global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __restrict__ cell,
+                                                          uint32_t* __restrict__ slot,
+                                                          const uint32_t* __restrict__ orig,
+                                                          const uint32_t* __restrict__ offset, uint32_t* tmp,
+                                                          uint32_t* count, uint32_t n, uint32_t* tile_sum,
+                                                          uint32_t n_tiles) {
+  pdl_wait();
+  scatter_block<false>(blockIdx.x, cell, slot, orig, offset, tmp, count, n, tile_sum, n_tiles);
+}
+
 // Canonical position = offset[c] + #{members of c with a smaller orig id};
 // moves the integrated state (P1, V1) there as (P0, V0) with its orig id.
-template <class T>
-__global__ void __launch_bounds__(STEP_THREADS) k_rank_move(StepBufs<T> b) {
-  pdl_wait();
-  const uint32_t base = blockIdx.x * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
+template <class T, bool COH>
+__device__ __forceinline__ void rank_move_block(uint32_t blk, const StepBufs<T>& b) {
+  const uint32_t base = blk * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
   uint32_t c[MOVE_PER_THREAD], sl[MOVE_PER_THREAD];
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
@@ -272,7 +280,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_rank_move(StepBufs<T> b) {
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     const uint32_t p = base + k * STEP_THREADS;
     if (p >= b.n) continue;
-    const uint32_t start = __ldg(b.offset + c[k]), end = __ldg(b.offset + c[k] + 1);
+    const uint32_t start = ld_ro<COH>(b.offset + c[k]), end = ld_ro<COH>(b.offset + c[k] + 1);
     const uint32_t o = b.tmp[start + sl[k]];
     uint32_t rank = 0;
     for (uint32_t s = start; s < end; ++s) rank += (b.tmp[s] < o) ? 1u : 0u;
@@ -282,6 +290,12 @@ __global__ void __launch_bounds__(STEP_THREADS) k_rank_move(StepBufs<T> b) {
     b.orig[d] = o;
     b.scell[d] = c[k];
   }
+}
+
+template <class T>
+__global__ void __launch_bounds__(STEP_THREADS) k_rank_move(StepBufs<T> b) {
+  pdl_wait();
+  rank_move_block<T, false>(blockIdx.x, b);
 }
 
 // ---- sphere-sphere contacts (ParticleModel_kernels.cu:136-201) --------------

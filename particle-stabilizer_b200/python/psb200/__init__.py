@@ -27,7 +27,7 @@ EXPORTED = (
     "ps_grid_get", "ps_buckets_get", "ps_last_launch_count", "ps_destroy", "ps_simulate",
     "ps_exclusive_scan_scratch_bytes", "ps_exclusive_scan_u32", "ps_read_csv", "ps_write_csv", "ps_read_obj",
     "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "ps_forward_checkpointed",
-    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_autotune", "ps_resolve_overlaps", "ps_overlap_stats",
+    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_autotune", "ps_set_neighbor_lists", "ps_list_stats", "ps_resolve_overlaps", "ps_overlap_stats",
     "ps_write_obj_spheres", "runSimulateCUDA",
 )
 KERNEL_KINDS = ("begin", "scan", "scatter", "rank_move", "contacts")
@@ -104,6 +104,8 @@ def lib() -> C.CDLL:
         L.ps_forward_checkpointed.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
         L.ps_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ps_exclusive_scan_u32_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        L.ps_set_neighbor_lists.argtypes = [C.c_void_p, C.c_double, C.c_int32]
+        L.ps_list_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.ps_resolve_overlaps.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int64),
                                           C.POINTER(C.c_double)]
         L.ps_overlap_stats.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
@@ -232,6 +234,21 @@ class Simulation:
     def forward_checkpointed(self, n_steps: int, every: int) -> None:
         """Advance n_steps keeping a checkpoint every `every` steps (for backward)."""
         _check(lib().ps_forward_checkpointed(self.h, int(n_steps), int(every)), "ps_forward_checkpointed")
+
+    def set_neighbor_lists(self, skin_fraction: float = 0.3, max_neighbours: int = 48) -> None:
+        """Neighbour-list mode (ps_set_neighbor_lists); 0 switches it off."""
+        _check(lib().ps_set_neighbor_lists(self.h, float(skin_fraction), int(max_neighbours)),
+               "ps_set_neighbor_lists")
+
+    def list_stats(self) -> tuple[int, int]:
+        """(rebuilds, fallbacks) since set_neighbor_lists (ps_list_stats)."""
+        r, f = C.c_int64(), C.c_int64()
+        _check(lib().ps_list_stats(self.h, C.byref(r), C.byref(f)), "ps_list_stats")
+        return int(r.value), int(f.value)
+
+    def list_fallbacks(self) -> int:
+        """ps_step calls repeated on the grid path after a list overflow."""
+        return self.list_stats()[1]
 
     def autotune(self, trial_steps: int = 20, cell_factors=(1.0, 1.05, 1.25, 1.5, 2.0),
                  graph_blocks=(50, 100, 200)) -> dict:

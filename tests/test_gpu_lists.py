@@ -1,0 +1,130 @@
+"""Neighbour-list mode (ps_set_neighbor_lists) against the grid path: the
+same scenes, stepped in the same calls, must give the same state bit for bit
+in FP32 and FP64 -- stable and diverging scenes, batches, triangle
+containers, lists rebuilt almost every step, and calls that overflow the
+lists and are repeated on the grid path."""
+import numpy as np
+import pytest
+
+import psb200
+from psb200 import scenes
+from oracle import ps_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CALLS = (1, 37, 200, 63)  # one-step call, a graph block and ragged remainders
+
+
+def run(scene, prec, calls=CALLS, skin=None, cap=48):
+    with psb200.Simulation(scene, prec) as sim:
+        sim.set_state()
+        if skin is not None:
+            sim.set_neighbor_lists(skin, cap)
+        for n in calls:
+            sim.step(n)
+        return sim.get_state(), (sim.list_stats() if skin is not None else (0, 0))
+
+
+def same(a, b):
+    return a.shape == b.shape and np.array_equal(a, b, equal_nan=True)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("make", [lambda: scenes.pile(1500, seed=11, k_spring=1.0),
+                                  lambda: scenes.settle_pile(side=10),
+                                  lambda: scenes.lattice_c1(side=12)],
+                         ids=["pile", "settle", "lattice"])
+def test_lists_equal_grid(need_gpu, make, prec):
+    sc = make()
+    want, _ = run(sc, prec)
+    got, (_, fb) = run(sc, prec, skin=0.3)
+    assert fb == 0
+    assert same(got, want)
+
+
+def test_lists_equal_oracle(need_gpu):
+    sc = scenes.pile(800, seed=12, k_spring=1.0)
+    got, (_, fb) = run(sc, "f32", calls=(90, 30), skin=0.25)
+    assert fb == 0
+    assert np.array_equal(got.astype(np.float32), O.run(sc, 120, "f32"))
+
+
+@pytest.mark.parametrize("skin", [0.02, 1.0])
+def test_lists_skin_extremes(need_gpu, skin):
+    # a thin skin makes the device ask for rebuilds inside the calls; a
+    # full-cell skin reaches two cells out
+    sc = scenes.pile(1200, seed=13, k_spring=1.0)
+    want, _ = run(sc, "f32")
+    got, (rebuilds, fb) = run(sc, "f32", skin=skin, cap=160)
+    assert fb == 0
+    # rebuilds inside the calls: the gated cooperative rebuild kernel ran
+    assert rebuilds > 0 or skin > 0.1
+    assert same(got, want)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_lists_diverging_scene(need_gpu, prec):
+    # spring 1e4 with dt 1e-5: k dt / m >> 1, the scene goes non-finite
+    sc = scenes.pile(1000, seed=14, k_spring=1e4)
+    want, _ = run(sc, prec, calls=(150, 150))
+    assert not np.isfinite(want).all()
+    got, _ = run(sc, prec, calls=(150, 150), skin=0.3, cap=200)
+    assert same(got, want)
+
+
+def test_lists_batch(need_gpu):
+    batch = [scenes.pile(300, seed=15, k_spring=0.5), scenes.settle_pile(side=8),
+             scenes.pile(900, seed=16, k_spring=2.0), scenes.pile(64, seed=17, k_spring=1e4)]
+    for prec in ("f32", "f64"):
+        want, _ = run(batch, prec)
+        got, _ = run(batch, prec, skin=0.4)
+        assert same(got, want)
+
+
+@pytest.mark.parametrize("make", [lambda: scenes.box_mesh_scene(), lambda: scenes.funnel_wall_scene(1500)],
+                         ids=["box_mesh", "funnel"])
+def test_lists_triangle_containers(need_gpu, make):
+    sc = make()
+    want, _ = run(sc, "f32", calls=(120, 80))
+    got, (_, fb) = run(sc, "f32", calls=(120, 80), skin=0.3)
+    assert fb == 0
+    assert same(got, want)
+
+
+def test_list_overflow_repeats_call_on_grid(need_gpu):
+    sc = scenes.pile(1000, seed=18, k_spring=1.0)
+    want, _ = run(sc, "f32", calls=(50, 50))
+    got, (_, fb) = run(sc, "f32", calls=(50, 50), skin=0.3, cap=2)
+    assert fb == 2
+    assert same(got, want)
+
+
+def test_lists_switch_on_and_off(need_gpu):
+    sc = scenes.pile(1200, seed=19, k_spring=1.0)
+    want, _ = run(sc, "f64", calls=(40, 40, 40, 40))
+    with psb200.Simulation(sc, "f64") as sim:
+        sim.set_state()
+        sim.set_neighbor_lists(0.3, 48)
+        sim.step(40)
+        sim.set_neighbor_lists(0.0, 0)
+        sim.step(40)
+        sim.set_neighbor_lists(0.5, 64)  # new capacity: new buffers and graphs
+        sim.step(40)
+        st = sim.stats(0)  # regrids from the at-rest state
+        assert np.isfinite(st.kinetic_energy) and st.kinetic_energy > 0.0
+        sim.step(40)
+        got = sim.get_state()
+    assert same(got, want)
+
+
+def test_list_arguments(need_gpu):
+    sc = scenes.pile(100, seed=20)
+    with psb200.Simulation(sc, "f32") as sim:
+        sim.set_state()
+        for bad in (1.5, 0.005, -0.1, float("nan")):
+            with pytest.raises(psb200.PSError, match="skin_fraction"):
+                sim.set_neighbor_lists(bad, 32)
+        with pytest.raises(psb200.PSError, match="max_neighbours"):
+            sim.set_neighbor_lists(0.3, 0)
+        sim.set_neighbor_lists(0.0, 0)
+        assert sim.list_stats() == (0, 0)
