@@ -17,12 +17,13 @@
 //
 // Rebuilds.  The step kernel also integrates the next step (as the fused
 // k_contacts) and tests whether some sphere has moved more than about
-// skin / 2 from where the lists were built.  The last block of the kernel to
-// finish writes the grid-wide answer to a gate word.  Before each step a
-// cooperative kernel, one wave of CTAs, reads the gate: closed, it returns
-// at once (about a microsecond; a conditional graph node costs ten);
-// open, it runs count, scan, scatter, rank/move and list build as phases
-// separated by grid barriers.  A list longer than the capacity, or a sphere
+// skin / 2 from where the lists were built; warps that see one set a flag
+// word of the next step's parity.  Before each step a cooperative kernel,
+// one wave of CTAs, reads that word: clear, it returns at once (about a
+// microsecond; a conditional graph node costs ten); set, it runs count,
+// scan, scatter, rank/move and list build as phases separated by grid
+// barriers.  The step kernel clears the word of its own parity, which that
+// kernel has read, for the step after next.  A list longer than the capacity, or a sphere
 // whose overlapping pairs change order and outnumber the sort buffer, sets
 // PS_DEVERR_LIST_OVERFLOW, and a barrier that waits too long sets
 // PS_DEVERR_LIST_BARRIER; the host then repeats the call on the grid path.
@@ -37,14 +38,21 @@ constexpr int LIST_CONTACTS_MAX = 32;  // sort buffer: overlapping pairs of a sp
 // words of ListBufs::flag; the first LIST_RESET_WORDS are zeroed when a
 // graph of steps starts
 enum : int {
-  LIST_MOVED = 0,     // some sphere of the running step moved too far
-  LIST_DONE = 1,      // CTAs of the running step kernel that finished
-  LIST_GATE = 2,      // rebuild before the next step
-  LIST_BAR = 3,       // grid barrier: arrivals, generation (2 words)
-  LIST_RESET_WORDS = 5,
-  LIST_REBUILDS = 5,  // rebuilds in the running call
-  LIST_FLAG_WORDS = 6
+  LIST_MOVED = 0,     // [parity of a step]: rebuild before that step (2 words)
+  LIST_BAR = 2,       // grid barrier: arrivals, generation (2 words)
+  LIST_RESET_WORDS = 4,
+  LIST_REBUILDS = 4,  // rebuilds in the running call
+  LIST_FLAG_WORDS = 5
 };
+
+// List entries whose loads the step kernel issues together.  Measured on
+// 1M-sphere scenes: FP32 single-scene runs gain most from 4; the batch
+// variant (scene lookup) spills at 4 and is fastest at 2; FP64 spills at
+// 2 and above and is fastest at 1.
+template <class T, bool MULTI>
+__host__ __device__ constexpr int list_batch() {
+  return sizeof(T) == 4 ? (MULTI ? 2 : 4) : 1;
+}
 
 constexpr uint32_t LIST_BARRIER_SPIN_LIMIT = 1u << 22;  // x >= 64 ns sleeps: a wait of 0.25 s or more
 
@@ -174,7 +182,8 @@ template <class T, bool MULTI>
 __global__ void __launch_bounds__(STEP_THREADS) k_list_rebuild(StepBufs<T> b, SceneParams<T> sp0, ListBufs<T> L,
                                                                int par, int64_t n_cells, uint32_t scan_tiles,
                                                                uint32_t scatter_blocks, uint32_t move_blocks) {
-  if (L.flag[LIST_GATE] == 0u || (*b.err & PS_DEVERR_LIST_BARRIER) != 0u) return;
+  if (L.flag[LIST_MOVED + par] == 0u || (*b.err & PS_DEVERR_LIST_BARRIER) != 0u) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(L.flag + LIST_REBUILDS, 1u);
   uint32_t* bar = L.flag + LIST_BAR;
   for (uint32_t base = blockIdx.x * STEP_THREADS; base < b.n; base += gridDim.x * STEP_THREADS) {
     const uint32_t p = base + threadIdx.x;
@@ -220,14 +229,19 @@ __device__ __forceinline__ bool list_pair(const ListBufs<T>& L, const StepBufs<T
 
 // One step on the lists: contacts of the step held in buffer `src`, then
 // (FUSED) the next step's integrate + container + cell id into buffer
-// 1 - src, the displacement test and the gate of the next step's rebuild;
-// the last step of a call (not FUSED) writes the at-rest state (P0
-// positions, V1 velocities) instead.
+// 1 - src and the displacement test, whose warps set the flag word of the
+// next step; the last step of a call (not FUSED) writes the at-rest state
+// (P0 positions, V1 velocities) instead.  Every load a sphere needs is
+// issued up front, and list entries list_batch() at a time, so that each
+// thread keeps several memory requests in flight.
 template <class T, bool MULTI, bool MESH, bool FUSED>
 __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 4 : 3)
     k_contacts_list(StepBufs<T> b, SceneParams<T> sp0, const MeshView* mv, ListBufs<T> L, int src) {
   pdl_wait();
   const int dst = 1 - src;
+  // this step's flag was read by the rebuild before it; clear it for the
+  // step after next
+  if (blockIdx.x == 0 && threadIdx.x == 0) L.flag[LIST_MOVED + src] = 0u;
   const uint32_t i = blockIdx.x * STEP_THREADS + threadIdx.x;
   const bool valid = i < b.n;
   bool moved = false;
@@ -236,29 +250,41 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 4 : 3)
     const vec4_t<T>* __restrict__ Ps = L.P[src];
     vec4_t<T> P = Ps[i];
     const vec4_t<T> Vi = L.V[src][i];
+    const uint32_t ci = L.cell[src][i];
+    const uint32_t nl = L.cnt[i];
+    vec4_t<T> R{};
+    if (FUSED) R = L.ref[i];
     T vx = Vi.x, vy = Vi.y, vz = Vi.z;
     int32_t cx, cy, cz;
-    cell_coords<T>(L.cell[src][i], sp, cx, cy, cz);
+    cell_coords<T>(ci, sp, cx, cy, cz);
     const bool live = isfinite(P.x) && isfinite(P.y) && isfinite(P.z);
-    if (live) {
+    if (live && nl > 0u) {
       const T ks = sp.k_spring, es = sp.e_sphere;
-      const uint32_t nl = L.cnt[i];
       // The list is in ascending (cell, original id) at the build; while
       // the overlapping pairs still come in ascending keys they are applied
       // in list order.
       uint64_t last = 0;
       bool ordered = true;
-      for (uint32_t k = 0; k < nl; ++k) {
-        const uint32_t j = L.list[(size_t)k * b.n + i];
-        const vec4_t<T> Q = ld4<T>(Ps + j);
-        uint64_t kj;
-        if (!list_pair<T>(L, b, sp, src, P, Q, j, cx, cy, cz, kj)) continue;
-        if (kj < last) {
-          ordered = false;
-          break;
+      constexpr int NB = list_batch<T, MULTI>();
+      for (uint32_t k0 = 0; k0 < nl && ordered; k0 += NB) {
+        uint32_t jj[NB];
+        vec4_t<T> QQ[NB];
+#pragma unroll
+        for (int u = 0; u < NB; ++u) jj[u] = k0 + u < nl ? L.list[(size_t)(k0 + u) * b.n + i] : i;
+#pragma unroll
+        for (int u = 0; u < NB; ++u) QQ[u] = ld4<T>(Ps + jj[u]);
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+          uint64_t kj;
+          if (k0 + u < nl && ordered && list_pair<T>(L, b, sp, src, P, QQ[u], jj[u], cx, cy, cz, kj)) {
+            if (kj < last) {
+              ordered = false;
+            } else {
+              last = kj;
+              contact_one<T>(L.V[src], jj[u], P, Vi, QQ[u], ks, es, vx, vy, vz);
+            }
+          }
         }
-        last = kj;
-        contact_one<T>(L.V[src], j, P, Vi, Q, ks, es, vx, vy, vz);
       }
       if (!ordered) {
         // some neighbour changed cells since the build: sort the
@@ -310,7 +336,6 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 4 : 3)
       // rebuild when the sphere is near half the skin from the build
       // position, or finite again after a non-finite build position; a
       // non-finite position takes part in no contact and asks for nothing
-      const vec4_t<T> R = L.ref[i];
       const T ex = P.x - R.x, ey = P.y - R.y, ez = P.z - R.z;
       const T half = T(0.49) * L.skin_frac * sp.interval;
       const bool fin = isfinite(P.x) && isfinite(P.y) && isfinite(P.z);
@@ -320,23 +345,7 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 4 : 3)
       b.V1[i] = V;
     }
   }
-  if constexpr (FUSED) {
-    // grid-wide OR of `moved`: every block adds its part and counts itself
-    // done; the last block reads the result into the gate and clears both
-    // words for the next step (nothing waits)
-    const int any = __syncthreads_or(moved ? 1 : 0);
-    if (threadIdx.x == 0) {
-      if (any) atomicOr(L.flag + LIST_MOVED, 1u);
-      __threadfence();
-      if (atomicAdd(L.flag + LIST_DONE, 1u) == gridDim.x - 1u) {
-        __threadfence();
-        const uint32_t f = atomicExch(L.flag + LIST_MOVED, 0u);
-        atomicExch(L.flag + LIST_DONE, 0u);
-        atomicExch(L.flag + LIST_GATE, f != 0u ? 1u : 0u);
-        if (f != 0u) atomicAdd(L.flag + LIST_REBUILDS, 1u);
-      }
-    }
-  }
+  if (FUSED && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31u) == 0u) atomicOr(L.flag + LIST_MOVED + dst, 1u);
 }
 
 }  // namespace psb
