@@ -25,6 +25,7 @@ from the reference sources) on the same scene and prints its line.
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -321,6 +322,51 @@ def mesh_measure(psb200, scenes_mod, device, steps: int) -> dict:
             "particles_below_rim_at_end": below_rim, "non_finite_at_end": non_finite(st)}
 
 
+def lists_measure(psb200, scenes_mod, device) -> dict:
+    """Neighbour-list mode against the grid path on the same steps from the
+    same state (after 100 warm-up steps), with the final states compared
+    bit for bit.  The skin fraction is chosen by ps_tune_neighbor_lists
+    (100 trial steps per candidate, 0 = grid path) from that state.
+    Scenes: 1M spheres with a soft spring (FP32 and FP64), the 1M-sphere
+    pile of the differentiation scene with spring 5, the 256 soft batch
+    scenes, and the 1M scene as specified, which diverges."""
+    cases = [("c2_1M_k0.25_fp32", lambda: scenes_mod.c2_scene(k_spring=0.25), "f32", 1000),
+             ("c2_1M_k0.25_fp64", lambda: scenes_mod.c2_scene(k_spring=0.25), "f64", 1000),
+             ("c4_1M_k5_fp32", lambda: scenes_mod.c4_scene(1 << 20, edge=0.95, k_spring=5.0), "f32", 1000),
+             ("c5_256_soft_fp32", lambda: scenes_mod.c5_scenes(256, k_range=(0.25, 2.5)), "f32", 300),
+             ("c2_1M_as_specified_fp32", lambda: scenes_mod.c2_scene(), "f32", 200)]
+    skins = (0.0, 0.02, 0.05, 0.1, 0.2)
+    out = {}
+    for name, make, prec, steps in cases:
+        sc = make()
+        n = sc.n if not isinstance(sc, list) else sum(x.n for x in sc)
+        with psb200.Simulation(sc, prec, device=device) as sim:
+            sim.set_state()
+            sim.step(100)
+            sim.checkpoint_save(1)
+            sim.time_steps(steps)
+            sim.checkpoint_load(1)
+            grid_ms = sim.time_steps(steps)
+            want = hashlib.sha256(sim.get_state().tobytes()).hexdigest()
+            sim.checkpoint_load(1)
+            tune = sim.tune_neighbor_lists(trial_steps=100, skins=skins, max_neighbours=64)
+            skin = tune["skin_fraction"]
+            sim.time_steps(steps)
+            sim.checkpoint_load(1)
+            rb0, fb0 = sim.list_stats()
+            list_ms = sim.time_steps(steps)
+            launches = sim.launches()
+            got = hashlib.sha256(sim.get_state().tobytes()).hexdigest()
+            rebuilds, fallbacks = (a - b for a, b in zip(sim.list_stats(), (rb0, fb0)))
+        out[name] = {"n_particles": n, "precision": prec, "skin_fraction": skin, "steps": steps,
+                     "tuning_skins": list(skins), "tuning_ms_per_step": tune["ms_table"],
+                     "grid_us_per_step": 1000.0 * grid_ms / steps, "list_us_per_step": 1000.0 * list_ms / steps,
+                     "speedup": grid_ms / list_ms, "identical_to_grid": got == want, "rebuilds": rebuilds,
+                     "fallbacks": fallbacks, "launches": launches,
+                     "list_particle_steps_per_s": n * steps / (list_ms * 1e-3)}
+    return out
+
+
 # Secondary measurements.  The reference's contact kick k*overlap/m is not
 # scaled by dt, so the scheme is stable only for k*dt/m below about 1.  The
 # differentiation and batch scenes with their specified springs (k*dt/m = 373
@@ -339,6 +385,7 @@ EXTRAS = {
                                                 k_range=(0.25, 2.5), tune=True),
     "batch_as_specified": lambda p, s, dev, a: batch_measure(p, s, dev, 100, 256, sequential=not a.no_sequential),
     "mesh": lambda p, s, dev, a: mesh_measure(p, s, dev, 20000),
+    "lists": lambda p, s, dev, a: lists_measure(p, s, dev),
 }
 
 

@@ -208,12 +208,22 @@ int ps_backward(ps_sim* sim, const double* dl_dstate, ps_grad* grads, double* dl
  * sphere are applied in the grid walk's order.  A list longer than
  * max_neighbours, or more than 32 overlapping pairs on one sphere whose
  * order changed since the build, makes ps_step repeat the whole call on the
- * grid path from its starting state.  In this mode ps_step returns after the
- * device has finished.
- * ps_list_stats: rebuilds requested by the device and calls repeated on the
- * grid path, both counted from the last ps_set_neighbor_lists. */
+ * grid path from its starting state.  When the device rebuilds more often
+ * than once per 4 steps over 256 or more steps, the next 1,024 steps run on
+ * the grid path (doubling, up to 65,536, while that repeats); both paths
+ * give the same states.  In this mode ps_step returns after the device has
+ * finished.
+ * ps_list_stats: rebuilds requested by the device, calls repeated on the
+ * grid path after an overflow, and steps run on the grid path by the
+ * backoff, all counted from the last ps_set_neighbor_lists; null pointers
+ * are skipped. */
 int ps_set_neighbor_lists(ps_sim* sim, double skin_fraction, int32_t max_neighbours);
-int ps_list_stats(ps_sim* sim, int64_t* rebuilds, int64_t* fallbacks);
+int ps_list_stats(ps_sim* sim, int64_t* rebuilds, int64_t* fallbacks, int64_t* grid_steps);
+/* Times trial_steps steps from the current state for every skin fraction in
+ * skins[n_skins] (0 = the grid path), writes ms per step to ms_table (may be
+ * null), keeps the fastest (ps_set_neighbor_lists) and restores the state. */
+int ps_tune_neighbor_lists(ps_sim* sim, int64_t trial_steps, const double* skins, int32_t n_skins,
+                           int32_t max_neighbours, double* ms_table, double* best_skin);
 
 typedef struct ps_tune_result {
   double cell_factor;        /* chosen f                                          */

@@ -131,6 +131,10 @@ struct ps_sim {
   void* list_ckpt = nullptr;              // state at the start of a list-mode call
   int64_t list_fallbacks = 0;             // calls repeated on the grid path after an overflow
   int64_t list_rebuilds = 0;              // grid + list rebuilds requested by the device
+  int64_t list_grid_steps = 0;            // list-mode steps run on the grid path (backoff)
+  // backoff: a window of list steps that rebuilt more than once per
+  // LIST_BACKOFF_RATE steps sends the next `list_backoff` steps to the grid path
+  int64_t list_win_steps = 0, list_win_rebuilds = 0, list_backoff = 0, list_backoff_len = 0;
   unsigned list_rebuild_grid = 0;         // CTAs of the cooperative rebuild (one wave)
 };
 
@@ -1253,6 +1257,14 @@ int step_graphs(ps_sim* s, int64_t n_steps, bool lists) {
   return PS_OK;
 }
 
+// A rebuild costs a few list steps; when a window of at least
+// LIST_BACKOFF_WINDOW list steps rebuilt more often than once per
+// LIST_BACKOFF_RATE steps (a scene moving fast against its skin, or
+// diverging), the following steps run on the grid path, for a stretch that
+// doubles while this repeats.
+constexpr int64_t LIST_BACKOFF_WINDOW = 256, LIST_BACKOFF_RATE = 4, LIST_BACKOFF_MIN = 1024,
+                  LIST_BACKOFF_MAX = 65536;
+
 // Neighbour-list path: exact as long as no list or overlap buffer overflows
 // (checked after the call); otherwise the call is repeated on the grid path
 // from the state it started from.
@@ -1292,6 +1304,18 @@ int step_lists(ps_sim* s, int64_t n_steps) {
   PS_CUDA(cudaMemcpyAsync(&nr, rebuilds, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
   PS_CUDA(cudaStreamSynchronize(s->stream));
   s->list_rebuilds += nr;
+  s->list_win_steps += n_steps;
+  s->list_win_rebuilds += nr;
+  if (s->list_win_steps >= LIST_BACKOFF_WINDOW) {
+    if (s->list_win_rebuilds * LIST_BACKOFF_RATE > s->list_win_steps) {
+      s->list_backoff_len = std::min<int64_t>(std::max<int64_t>(2 * s->list_backoff_len, LIST_BACKOFF_MIN),
+                                              LIST_BACKOFF_MAX);
+      s->list_backoff = s->list_backoff_len;
+    } else {
+      s->list_backoff_len = 0;
+    }
+    s->list_win_steps = s->list_win_rebuilds = 0;
+  }
   constexpr uint32_t list_err = PS_DEVERR_LIST_OVERFLOW | PS_DEVERR_LIST_BARRIER;
   if (e & list_err) {
     // counts and tile totals may be left over from an interrupted rebuild
@@ -1332,13 +1356,16 @@ extern "C" int ps_set_neighbor_lists(ps_sim* s, double skin_fraction, int32_t ma
   s->list_cap = skin_fraction > 0.0 ? max_neighbours : 0;
   s->list_rebuilds = 0;
   s->list_fallbacks = 0;
+  s->list_grid_steps = 0;
+  s->list_win_steps = s->list_win_rebuilds = s->list_backoff = s->list_backoff_len = 0;
   return PS_OK;
 }
 
-extern "C" int ps_list_stats(ps_sim* s, int64_t* rebuilds, int64_t* fallbacks) {
+extern "C" int ps_list_stats(ps_sim* s, int64_t* rebuilds, int64_t* fallbacks, int64_t* grid_steps) {
   if (s == nullptr) return fail(PS_ERR_INVALID, "ps_list_stats: null simulation");
   if (rebuilds != nullptr) *rebuilds = s->list_rebuilds;
   if (fallbacks != nullptr) *fallbacks = s->list_fallbacks;
+  if (grid_steps != nullptr) *grid_steps = s->list_grid_steps;
   return PS_OK;
 }
 
@@ -1349,7 +1376,16 @@ extern "C" int ps_step(ps_sim* s, int64_t n_steps) {
   if (n_steps == 0 || s->n_total == 0) return PS_OK;
   DeviceGuard guard(s->device);
   const bool lists = s->list_skin > 0.0;
-  const int rc = lists ? step_lists(s, n_steps) : step_graphs(s, n_steps, false);
+  int rc = PS_OK;
+  int64_t left = n_steps;
+  if (lists && s->list_backoff > 0) {
+    const int64_t g = std::min(left, s->list_backoff);
+    rc = step_graphs(s, g, false);
+    s->list_backoff -= g;
+    s->list_grid_steps += g;
+    left -= g;
+  }
+  if (rc == PS_OK && left > 0) rc = lists ? step_lists(s, left) : step_graphs(s, left, false);
   if (rc != PS_OK) return rc;
   s->grid_valid = !lists;  // after the list path the grid arrays do not describe the at-rest state
   s->stepped = true;
@@ -1512,6 +1548,61 @@ extern "C" int ps_autotune(ps_sim* s, int64_t trial_steps, const double* cell_fa
   out->graph_block = best_l;
   out->ms_per_step = best;
   out->before_ms_per_step = before;
+  return PS_OK;
+}
+
+extern "C" int ps_tune_neighbor_lists(ps_sim* s, int64_t trial_steps, const double* skins, int32_t n_skins,
+                                      int32_t max_neighbours, double* ms_table, double* best_skin) {
+  if (s == nullptr || best_skin == nullptr || trial_steps < 1 || skins == nullptr || n_skins < 1 ||
+      max_neighbours < 1 || max_neighbours > 4096)
+    return fail(PS_ERR_INVALID, "ps_tune_neighbor_lists: bad argument");
+  for (int32_t k = 0; k < n_skins; ++k)
+    if (!(skins[k] == 0.0 || (skins[k] >= 0.01 && skins[k] <= 1.0)))
+      return fail(PS_ERR_INVALID, "ps_tune_neighbor_lists: each skin_fraction must be 0 or in [0.01, 1]");
+  if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_tune_neighbor_lists: call ps_set_state first");
+  DeviceGuard guard(s->device);
+  void* saved = nullptr;
+  int rc = save_state(s, saved);
+  if (rc != PS_OK) return rc;
+  cudaEvent_t ea, eb;
+  PS_CUDA(cudaEventCreate(&ea));
+  PS_CUDA(cudaEventCreate(&eb));
+  // one trial: the same steps twice from the saved state, the second timed
+  // (the first captures the graphs)
+  auto trial = [&](double skin, double& ms_per_step) -> int {
+    int r = ps_set_neighbor_lists(s, skin, max_neighbours);
+    if (r == PS_OK) r = load_state(s, saved);
+    if (r == PS_OK) r = ps_step(s, trial_steps);
+    if (r == PS_OK) r = load_state(s, saved);
+    if (r != PS_OK) return r;
+    cudaEventRecord(ea, s->stream);
+    r = ps_step(s, trial_steps);
+    cudaEventRecord(eb, s->stream);
+    if (cudaEventSynchronize(eb) != cudaSuccess) return fail(PS_ERR_CUDA, "ps_tune_neighbor_lists: timing failed");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ea, eb);
+    ms_per_step = (double)ms / (double)trial_steps;
+    if (r == PS_OK) r = check_device_error(s);
+    return r;
+  };
+  double best = INFINITY, best_k = skins[0];
+  for (int32_t k = 0; k < n_skins && rc == PS_OK; ++k) {
+    double ms = 0.0;
+    rc = trial(skins[k], ms);
+    if (ms_table != nullptr) ms_table[k] = ms;
+    if (rc == PS_OK && ms < best) {
+      best = ms;
+      best_k = skins[k];
+    }
+  }
+  if (rc == PS_OK) rc = ps_set_neighbor_lists(s, best_k, max_neighbours);
+  if (rc == PS_OK) rc = load_state(s, saved);
+  if (rc == PS_OK) rc = ps_sync(s);
+  cudaEventDestroy(ea);
+  cudaEventDestroy(eb);
+  cudaFree(saved);
+  if (rc != PS_OK) return rc;
+  *best_skin = best_k;
   return PS_OK;
 }
 

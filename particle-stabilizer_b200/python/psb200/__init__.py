@@ -27,7 +27,8 @@ EXPORTED = (
     "ps_grid_get", "ps_buckets_get", "ps_last_launch_count", "ps_destroy", "ps_simulate",
     "ps_exclusive_scan_scratch_bytes", "ps_exclusive_scan_u32", "ps_read_csv", "ps_write_csv", "ps_read_obj",
     "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "ps_forward_checkpointed",
-    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_autotune", "ps_set_neighbor_lists", "ps_list_stats", "ps_resolve_overlaps", "ps_overlap_stats",
+    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_autotune", "ps_set_neighbor_lists", "ps_list_stats", "ps_tune_neighbor_lists",
+    "ps_resolve_overlaps", "ps_overlap_stats",
     "ps_write_obj_spheres", "runSimulateCUDA",
 )
 KERNEL_KINDS = ("begin", "scan", "scatter", "rank_move", "contacts")
@@ -105,7 +106,9 @@ def lib() -> C.CDLL:
         L.ps_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ps_exclusive_scan_u32_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
         L.ps_set_neighbor_lists.argtypes = [C.c_void_p, C.c_double, C.c_int32]
-        L.ps_list_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ps_list_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ps_tune_neighbor_lists.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                                             C.c_void_p]
         L.ps_resolve_overlaps.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int64),
                                           C.POINTER(C.c_double)]
         L.ps_overlap_stats.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
@@ -242,9 +245,23 @@ class Simulation:
 
     def list_stats(self) -> tuple[int, int]:
         """(rebuilds, fallbacks) since set_neighbor_lists (ps_list_stats)."""
-        r, f = C.c_int64(), C.c_int64()
-        _check(lib().ps_list_stats(self.h, C.byref(r), C.byref(f)), "ps_list_stats")
-        return int(r.value), int(f.value)
+        return self.list_stats_all()[:2]
+
+    def list_stats_all(self) -> tuple[int, int, int]:
+        """(rebuilds, fallbacks, steps run on the grid path by the backoff)."""
+        r, f, g = C.c_int64(), C.c_int64(), C.c_int64()
+        _check(lib().ps_list_stats(self.h, C.byref(r), C.byref(f), C.byref(g)), "ps_list_stats")
+        return int(r.value), int(f.value), int(g.value)
+
+    def tune_neighbor_lists(self, trial_steps: int = 100, skins=(0.0, 0.02, 0.05, 0.1, 0.2),
+                            max_neighbours: int = 64) -> dict:
+        """ps_tune_neighbor_lists: the fastest skin fraction (0 = grid path)."""
+        sk = np.ascontiguousarray(skins, dtype=np.float64)
+        table = np.zeros(len(sk), dtype=np.float64)
+        best = C.c_double()
+        _check(lib().ps_tune_neighbor_lists(self.h, int(trial_steps), _ptr(sk), len(sk), int(max_neighbours),
+                                            _ptr(table), C.byref(best)), "ps_tune_neighbor_lists")
+        return {"skin_fraction": float(best.value), "skins": [float(x) for x in sk], "ms_table": table.tolist()}
 
     def list_fallbacks(self) -> int:
         """ps_step calls repeated on the grid path after a list overflow."""

@@ -72,6 +72,27 @@ def test_lists_diverging_scene(need_gpu, prec):
     assert same(got, want)
 
 
+def test_lists_back_off_to_grid_on_a_fast_scene(need_gpu):
+    # spheres that cross half the skin every step or two: after a window of
+    # 256 list steps the next 1,024 steps run on the grid path, with the same
+    # states
+    sc = scenes.pile(1000, seed=21, k_spring=1.0)
+    st = sc.state.copy()
+    st[:, 3:6] *= 50.0
+    sc = sc.copy(state=st)
+    calls = (150, 150, 150, 150)
+    want, _ = run(sc, "f32", calls=calls)
+    with psb200.Simulation(sc, "f32") as sim:
+        sim.set_state()
+        sim.set_neighbor_lists(0.01, 200)
+        for n in calls:
+            sim.step(n)
+        got = sim.get_state()
+        rebuilds, _, grid_steps = sim.list_stats_all()
+    assert rebuilds * 4 > 300 and grid_steps == 300
+    assert same(got, want)
+
+
 def test_lists_batch(need_gpu):
     batch = [scenes.pile(300, seed=15, k_spring=0.5), scenes.settle_pile(side=8),
              scenes.pile(900, seed=16, k_spring=2.0), scenes.pile(64, seed=17, k_spring=1e4)]
@@ -117,6 +138,26 @@ def test_lists_switch_on_and_off(need_gpu):
     assert same(got, want)
 
 
+def test_tune_neighbor_lists_restores_state_and_keeps_parity(need_gpu):
+    sc = scenes.pile(1500, seed=22, k_spring=1.0)
+    want, _ = run(sc, "f32", calls=(60,))
+    with psb200.Simulation(sc, "f32") as sim:
+        sim.set_state()
+        before = sim.get_state()
+        res = sim.tune_neighbor_lists(trial_steps=20, skins=(0.0, 0.05, 0.3), max_neighbours=96)
+        assert len(res["ms_table"]) == 3 and all(t > 0 for t in res["ms_table"])
+        assert res["skin_fraction"] == res["skins"][int(np.argmin(res["ms_table"]))]
+        assert np.array_equal(sim.get_state(), before)
+        assert sim.list_stats_all() == (0, 0, 0)
+        sim.step(60)
+        got = sim.get_state()
+    assert same(got, want)
+    with psb200.Simulation(sc, "f32") as sim:
+        sim.set_state()
+        with pytest.raises(psb200.PSError, match="skin_fraction"):
+            sim.tune_neighbor_lists(trial_steps=5, skins=(0.005,))
+
+
 def test_list_arguments(need_gpu):
     sc = scenes.pile(100, seed=20)
     with psb200.Simulation(sc, "f32") as sim:
@@ -127,4 +168,4 @@ def test_list_arguments(need_gpu):
         with pytest.raises(psb200.PSError, match="max_neighbours"):
             sim.set_neighbor_lists(0.3, 0)
         sim.set_neighbor_lists(0.0, 0)
-        assert sim.list_stats() == (0, 0)
+        assert sim.list_stats_all() == (0, 0, 0)
