@@ -322,11 +322,13 @@ def mesh_measure(psb200, scenes_mod, device, steps: int) -> dict:
             "particles_below_rim_at_end": below_rim, "non_finite_at_end": non_finite(st)}
 
 
-def lists_measure(psb200, scenes_mod, device) -> dict:
+def lists_measure(psb200, scenes_mod, device, only=None, fixed_skin=None) -> dict:
     """Neighbour-list mode against the grid path on the same steps from the
     same state (after 100 warm-up steps), with the final states compared
     bit for bit.  The skin fraction is chosen by ps_tune_neighbor_lists
-    (100 trial steps per candidate, 0 = grid path) from that state.
+    (100 trial steps per candidate, 0 = grid path) from that state, unless
+    `fixed_skin` gives it (profiling runs, where the tuner's timings mean
+    nothing).
     Scenes: 1M spheres with a soft spring (FP32 and FP64), the 1M-sphere
     pile of the differentiation scene with spring 5, the 256 soft batch
     scenes, and the 1M scene as specified, which diverges."""
@@ -338,6 +340,8 @@ def lists_measure(psb200, scenes_mod, device) -> dict:
     skins = (0.0, 0.02, 0.05, 0.1, 0.2)
     out = {}
     for name, make, prec, steps in cases:
+        if only is not None and name != only:
+            continue
         sc = make()
         n = sc.n if not isinstance(sc, list) else sum(x.n for x in sc)
         with psb200.Simulation(sc, prec, device=device) as sim:
@@ -349,8 +353,13 @@ def lists_measure(psb200, scenes_mod, device) -> dict:
             grid_ms = sim.time_steps(steps)
             want = hashlib.sha256(sim.get_state().tobytes()).hexdigest()
             sim.checkpoint_load(1)
-            tune = sim.tune_neighbor_lists(trial_steps=100, skins=skins, max_neighbours=64)
-            skin = tune["skin_fraction"]
+            if fixed_skin is None:
+                tune = sim.tune_neighbor_lists(trial_steps=100, skins=skins, max_neighbours=64)
+                skin = tune["skin_fraction"]
+            else:
+                tune = {"ms_table": None}
+                skin = fixed_skin
+                sim.set_neighbor_lists(skin, 64)
             sim.time_steps(steps)
             sim.checkpoint_load(1)
             rb0, fb0 = sim.list_stats()
@@ -385,7 +394,7 @@ EXTRAS = {
                                                 k_range=(0.25, 2.5), tune=True),
     "batch_as_specified": lambda p, s, dev, a: batch_measure(p, s, dev, 100, 256, sequential=not a.no_sequential),
     "mesh": lambda p, s, dev, a: mesh_measure(p, s, dev, 20000),
-    "lists": lambda p, s, dev, a: lists_measure(p, s, dev),
+    "lists": lambda p, s, dev, a: lists_measure(p, s, dev, a.scene, a.skin),
 }
 
 
@@ -528,6 +537,10 @@ def main():
                     help="run only this secondary measurement on the local GPU and print its JSON")
     ap.add_argument("--no-sequential", action="store_true",
                     help="with --extra batch: skip the scene-by-scene comparison")
+    ap.add_argument("--scene", default=None,
+                    help="with --extra lists: measure only this scene (e.g. c2_1M_k0.25_fp32)")
+    ap.add_argument("--skin", type=float, default=None,
+                    help="with --extra lists: this skin fraction instead of the tuner's choice")
     args = ap.parse_args()
     if args.extra is not None:
         import psb200
