@@ -272,11 +272,22 @@ def batch_measure(psb200, scenes_mod, device, steps: int, n_scenes: int, sequent
             sim.time_steps(steps)
             sim.checkpoint_load(0)
             tuned_ms = sim.time_steps(steps)
+            tuned_hash = hashlib.sha256(sim.get_state().tobytes()).hexdigest()
+            # neighbour lists on the tuned grid, skin by ps_tune_neighbor_lists
+            sim.checkpoint_load(0)
+            lt = sim.tune_neighbor_lists(trial_steps=50, skins=(0.0, 0.02, 0.05, 0.1, 0.2))
+            sim.time_steps(steps)
+            sim.checkpoint_load(0)
+            lists_ms = sim.time_steps(steps)
+            lists = {"batched_ms": lists_ms, "skin_fraction": lt["skin_fraction"], "trial_skins": lt["skins"],
+                     "trial_ms_per_step": lt["ms_table"],
+                     "batched_particle_steps_per_s": n_total * steps / (lists_ms * 1e-3),
+                     "identical_to_tuned_grid": hashlib.sha256(sim.get_state().tobytes()).hexdigest() == tuned_hash}
             tuned = {"batched_ms": tuned_ms, "cell_factor": choice["cell_factor"],
                      "graph_block": choice["graph_block"], "trial_ms_table": choice["ms_table"],
                      "trial_cell_factors": choice["cell_factors"], "trial_graph_blocks": choice["graph_blocks"],
                      "batched_particle_steps_per_s": n_total * steps / (tuned_ms * 1e-3),
-                     "non_finite_at_end": non_finite(sim.get_state())}
+                     "non_finite_at_end": non_finite(sim.get_state()), "neighbor_lists": lists}
     out = {"n_scenes": n_scenes, "n_particles": n_total, "k_range": list(k_range), "steps": steps,
            "batched_ms": batched_ms,
            "batched_scene_steps_per_s": n_scenes * steps / (batched_ms * 1e-3),
@@ -300,6 +311,8 @@ def batch_measure(psb200, scenes_mod, device, steps: int, n_scenes: int, sequent
                 "speedup_batched_over_sequential": seq_ms / batched_ms, "launches_sequential": seq_launches})
     if "autotuned" in out:
         out["autotuned"]["speedup_over_sequential"] = seq_ms / out["autotuned"]["batched_ms"]
+        nl = out["autotuned"]["neighbor_lists"]
+        nl["speedup_over_sequential"] = seq_ms / nl["batched_ms"]
     return out
 
 

@@ -3,6 +3,9 @@ same scenes, stepped in the same calls, must give the same state bit for bit
 in FP32 and FP64 -- stable and diverging scenes, batches, triangle
 containers, lists rebuilt almost every step, and calls that overflow the
 lists and are repeated on the grid path."""
+import os
+import subprocess
+
 import numpy as np
 import pytest
 
@@ -169,3 +172,33 @@ def test_list_arguments(need_gpu):
             sim.set_neighbor_lists(0.3, 0)
         sim.set_neighbor_lists(0.0, 0)
         assert sim.list_stats_all() == (0, 0, 0)
+
+
+@pytest.mark.parametrize("setting", ["auto", "0.05"])
+def test_cli_with_neighbor_lists_writes_the_same_csv(need_gpu, tmp_path, setting):
+    """runSimulateCUDA with PSB200_NEIGHBOR_LISTS: the output CSV is the
+    grid path's, byte for byte."""
+    sc = scenes.pile(2000, seed=23, k_spring=1.0)
+    csv_in = tmp_path / "in.csv"
+    with open(csv_in, "w") as f:
+        f.write("x,y,z,r\n")
+        for p in sc.state:
+            f.write("%.17g,%.17g,%.17g,%.17g\n" % (p[0], p[1], p[2], p[6]))
+    outs = {}
+    for tag, env_value in (("grid", None), ("lists", setting)):
+        out = tmp_path / f"{tag}.csv"
+        cmd = [psb200.CLI_PATH, "--lib", psb200.LIB_PATH, str(csv_in), "--cuda", "--max-steps", "400",
+               "--box-min", *map(str, sc.box_min), "--box-max", *map(str, sc.box_max), "--dt", "1e-05",
+               "--coeff-of-spring", "1", "--coeff-of-restitution-sphere", "0.5",
+               "--coeff-of-restitution-wall", *["0.7"] * 6, "--gravity", "0", "0", "-9.8",
+               "--initial-velocity", "0.05", "0", "-0.1", "--density", "1000", "--out-csv-path", str(out)]
+        env = dict(os.environ)
+        env.pop("PSB200_NEIGHBOR_LISTS", None)
+        if env_value is not None:
+            env["PSB200_NEIGHBOR_LISTS"] = env_value
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
+        assert r.returncode == 0, r.stdout + r.stderr
+        if env_value is not None:
+            assert "neighbour-list skin" in r.stdout
+        outs[tag] = out.read_text()
+    assert outs["lists"] == outs["grid"]
