@@ -71,19 +71,30 @@ def test_head_to_head_with_reference_cuda_at_1m_spheres(need_gpu):
     build indexes out of range once positions stop being finite).  Both run
     steps 21..220 from the same initial state; the reference runs only after
     this library's FP64 run of the same steps stayed finite and inside the
-    box.  Target: at least 3x the reference's particle-steps/s."""
+    box.  Target: at least 3x the reference's particle-steps/s.  The same
+    steps are also timed with neighbour lists (skin by the tuner), whose
+    states must equal the grid path's."""
     import time
 
     sc = scenes.c2_scene(k_spring=0.25)
     warm, steps = 20, 200
-    ours = {}
+    ours, lists = {}, {}
     for prec in ("f32", "f64"):
         with psb200.Simulation(sc, prec) as sim:
             sim.set_state()
             sim.step(warm)
             ms = sim.time_steps(steps)
             st = sim.get_state()
+            sim.set_state()
+            sim.step(warm)
+            sim.checkpoint_save(0)
+            skin = sim.tune_neighbor_lists(trial_steps=50)["skin_fraction"]
+            sim.time_steps(steps)
+            sim.checkpoint_load(0)
+            ms_lists = sim.time_steps(steps)
+            assert np.array_equal(sim.get_state(), st)
         ours[prec] = sc.n * steps / (ms * 1e-3)
+        lists[prec] = (sc.n * steps / (ms_lists * 1e-3), skin)
         assert np.isfinite(st).all()
         assert np.all(st[:, :3] >= np.array(sc.box_min)) and np.all(st[:, :3] <= np.array(sc.box_max))
     r = O.ref_cuda()
@@ -99,7 +110,9 @@ def test_head_to_head_with_reference_cuda_at_1m_spheres(need_gpu):
     ref = sc.n * steps / ref_s
     print(f"\n1M spheres, steps {warm + 1}..{warm + steps}: reference CUDA (FP64) {ref:.3e} particle-steps/s "
           f"({1e3 * ref_s / steps:.3f} ms/step); this library FP64 {ours['f64']:.3e} ({ours['f64'] / ref:.1f}x), "
-          f"FP32 {ours['f32']:.3e} ({ours['f32'] / ref:.1f}x); reference set-up and warm-up "
+          f"FP32 {ours['f32']:.3e} ({ours['f32'] / ref:.1f}x); with neighbour lists FP64 {lists['f64'][0]:.3e} "
+          f"({lists['f64'][0] / ref:.1f}x, skin {lists['f64'][1]}), FP32 {lists['f32'][0]:.3e} "
+          f"({lists['f32'][0] / ref:.1f}x, skin {lists['f32'][1]}); reference set-up and warm-up "
           f"{time.perf_counter() - t0 - ref_s:.1f} s")
     assert ours["f64"] >= 3.0 * ref and ours["f32"] >= 3.0 * ref
 
