@@ -202,3 +202,24 @@ def test_cli_with_neighbor_lists_writes_the_same_csv(need_gpu, tmp_path, setting
             assert "neighbour-list skin" in r.stdout
         outs[tag] = out.read_text()
     assert outs["lists"] == outs["grid"]
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_adjoint_after_a_forward_on_lists(need_gpu, prec):
+    # ps_forward_checkpointed steps through ps_step, so with lists on its
+    # forward pass runs on them; checkpoints, final state and gradients must
+    # equal the grid path's bit for bit
+    sc = scenes.pile(1000, seed=24, k_spring=1.0)
+    out = {}
+    for skin in (None, 0.05):
+        with psb200.Simulation(sc, prec) as sim:
+            sim.set_state()
+            if skin is not None:
+                sim.set_neighbor_lists(skin, 64)
+            sim.forward_checkpointed(300, 50)
+            final = sim.get_state()
+            _, g = psb200.height_loss(final)
+            grads, g0 = sim.backward(g)
+            out[skin] = (final, grads[0], g0)
+    assert same(out[0.05][0], out[None][0])
+    assert np.array_equal(out[0.05][1], out[None][1]) and np.array_equal(out[0.05][2], out[None][2])
