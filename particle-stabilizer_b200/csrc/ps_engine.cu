@@ -118,6 +118,9 @@ struct ps_sim {
   std::map<int32_t, void*> checkpoints;  // slot -> device copy of (P0, V1, orig)
   cudaAccessPolicyWindow l2_window{};     // count + offset arrays kept in L2
   bool l2_window_on = false;
+  size_t l2_limit = 0;                    // persisting set-aside this simulation wants
+  size_t l2_prev_limit = 0;               // the context's set-aside before this simulation changed it
+  bool l2_limit_set = false;
   // differentiation
   int64_t fwd_steps = 0, fwd_every = 0;   // last ps_forward_checkpointed
   std::vector<void*> fwd_ckpt;            // state at the start of each block, + final state last
@@ -708,11 +711,14 @@ void setup_l2_window(ps_sim* s, size_t bytes) {
   const size_t win = std::min<size_t>(bytes, (size_t)prop.accessPolicyMaxWindowSize);
   size_t cur = 0;
   cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+  if (!s->l2_limit_set) s->l2_prev_limit = cur;
   const size_t want = std::min<size_t>((size_t)prop.persistingL2CacheMaxSize, win);
-  if (cur < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+  if (cur != want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
     cudaGetLastError();
     return;
   }
+  s->l2_limit = want;
+  s->l2_limit_set = true;
   cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
   s->l2_window.base_ptr = s->cell_arena;
   s->l2_window.num_bytes = win;
@@ -727,8 +733,22 @@ void setup_l2_window(ps_sim* s, size_t bytes) {
     cudaGetLastError();
 }
 
+// The set-aside is a limit of the whole context, and a larger one than the
+// running simulation's window takes L2 from its ordinary accesses (a 1M-sphere
+// step ran 20 % slower after a batch of large grids had raised it); each
+// call sets it back to this simulation's own size.
+void ensure_l2_limit(ps_sim* s) {
+  if (!s->l2_window_on) return;
+  size_t cur = 0;
+  if (cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize) == cudaSuccess && cur != s->l2_limit)
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, s->l2_limit);
+  cudaGetLastError();
+}
+
 // Captured kernel nodes carry the window explicitly.
-void apply_l2_window(ps_sim* s, cudaGraph_t g) {
+// `clear` gives the nodes an empty window instead (neighbour-list graphs:
+// their steps do not touch the cell arrays, which only a rebuild reads).
+void apply_l2_window(ps_sim* s, cudaGraph_t g, bool clear = false) {
   if (!s->l2_window_on) return;
   size_t n = 0;
   if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return;
@@ -736,6 +756,7 @@ void apply_l2_window(ps_sim* s, cudaGraph_t g) {
   cudaGraphGetNodes(g, nodes.data(), &n);
   cudaKernelNodeAttrValue v{};
   v.accessPolicyWindow = s->l2_window;
+  if (clear) v.accessPolicyWindow.num_bytes = 0;
   for (auto nd : nodes) {
     cudaGraphNodeType t;
     if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
@@ -882,6 +903,10 @@ void free_sim(ps_sim* s) {
     v.accessPolicyWindow.num_bytes = 0;
     cudaStreamSetAttribute(s->stream, cudaStreamAttributeAccessPolicyWindow, &v);
     cudaCtxResetPersistingL2Cache();
+    cudaGetLastError();
+  }
+  if (s->l2_limit_set) {  // give the context back the set-aside it had
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, s->l2_prev_limit);
     cudaGetLastError();
   }
   for (auto& kv : s->checkpoints) cudaFree(kv.second);
@@ -1243,7 +1268,7 @@ int step_graphs(ps_sim* s, int64_t n_steps, bool lists) {
         if (graph) cudaGraphDestroy(graph);
         return fail(PS_ERR_CUDA, std::string("ps_step: capture failed: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee));
       }
-      apply_l2_window(s, graph);
+      apply_l2_window(s, graph, lists);
       cudaGraphExec_t exec = nullptr;
       const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
       cudaGraphDestroy(graph);
@@ -1296,6 +1321,13 @@ int step_lists(ps_sim* s, int64_t n_steps) {
   uint32_t* rebuilds = s->precision == PS_FP32 ? list_bufs<float>(s).flag + LIST_REBUILDS
                                                : list_bufs<double>(s).flag + LIST_REBUILDS;
   PS_CUDA(cudaMemsetAsync(rebuilds, 0, sizeof(uint32_t), s->stream));
+  // the grid path's persisting lines (cell counts and offsets) would hold
+  // L2 that the list steps stream through
+  if (s->l2_window_on) {
+    PS_CUDA(cudaStreamSynchronize(s->stream));
+    cudaCtxResetPersistingL2Cache();
+    cudaGetLastError();
+  }
   int rc = save_state(s, s->list_ckpt);
   if (rc == PS_OK) rc = step_graphs(s, n_steps, true);
   if (rc != PS_OK) return rc;
@@ -1375,6 +1407,7 @@ extern "C" int ps_step(ps_sim* s, int64_t n_steps) {
   s->last_launches = 0;
   if (n_steps == 0 || s->n_total == 0) return PS_OK;
   DeviceGuard guard(s->device);
+  ensure_l2_limit(s);
   const bool lists = s->list_skin > 0.0;
   int rc = PS_OK;
   int64_t left = n_steps;
@@ -1664,6 +1697,7 @@ extern "C" int ps_backward(ps_sim* s, const double* dl_dstate, ps_grad* grads, d
   if (s == nullptr || dl_dstate == nullptr || grads == nullptr) return fail(PS_ERR_INVALID, "ps_backward: null argument");
   if (s->fwd_steps < 1) return fail(PS_ERR_INVALID, "ps_backward: call ps_forward_checkpointed first");
   DeviceGuard guard(s->device);
+  ensure_l2_limit(s);
   if (s->precision == PS_FP32)
     return s->multi ? backward_impl<float, true>(s, dl_dstate, grads, dl_dstate0)
                     : backward_impl<float, false>(s, dl_dstate, grads, dl_dstate0);
