@@ -98,6 +98,7 @@ struct ps_sim {
   void *P0 = nullptr, *V0 = nullptr, *P1 = nullptr, *V1 = nullptr;
   uint32_t *orig = nullptr, *cell = nullptr, *slot = nullptr, *tmp = nullptr, *scell = nullptr;
   uint32_t *count = nullptr, *offset = nullptr, *err = nullptr, *d_pbase = nullptr;
+  double* d_interval = nullptr;  // cell edge of each scene, for the device-side upload check
   uint32_t* tile_sum = nullptr;  // per-tile totals of `count` for the step's scan
   void* d_bounds = nullptr;       // per-scene, per-axis cell boundaries in the state precision
   double* staging = nullptr;  // n_total x 8 doubles
@@ -459,6 +460,25 @@ int check_device_error(ps_sim* s) {
 }
 
 // ---- conversion kernels between the host AoS and the device SoA ------------
+// Upload check of a new state against the grid sized by the first upload:
+// each particle must fit a cell (2 r <= cell edge of its scene) and have a
+// positive mass; the lowest failing index is kept in *bad (NaN fails too).
+__global__ void k_upload_check(const double* __restrict__ aos, const uint32_t* __restrict__ pbase, int n_scenes,
+                               const double* __restrict__ interval, uint32_t* bad, uint32_t n) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  int lo = 0, hi = n_scenes - 1;  // largest scene s with pbase[s] <= p
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pbase[mid] <= p)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const double r = aos[8 * (size_t)p + 6], m = aos[8 * (size_t)p + 7];
+  if (!(2.0 * r <= interval[lo]) || !(m > 0.0)) atomicMin(bad, p);
+}
+
 template <class T>
 __global__ void k_upload(const double* __restrict__ aos, vec4_t<T>* P0, vec4_t<T>* V1, uint32_t* orig, uint32_t n) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -866,6 +886,12 @@ int size_grids(ps_sim* s, const double* aos) {
   PS_CUDA(cudaMemset(s->cell_arena, 0, 2 * cells_b + tiles_b));
   setup_l2_window(s, 2 * cells_b + tiles_b);
 
+  {
+    std::vector<double> iv((size_t)s->n_scenes);
+    for (int sc = 0; sc < s->n_scenes; ++sc) iv[(size_t)sc] = s->grids[sc].interval;
+    PS_CUDA(cudaMemcpy(s->d_interval, iv.data(), 8 * iv.size(), cudaMemcpyHostToDevice));
+  }
+
   // scene parameter tables
   s->sp32.clear();
   s->sp64.clear();
@@ -1161,8 +1187,9 @@ extern "C" int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t 
   const size_t vb = s->precision == PS_FP32 ? 16 : 32;
   const size_t n = (size_t)std::max<int64_t>(s->n_total, 1);
   const size_t b4 = align_up(vb * n, 256), bu = align_up(4 * n, 256), bs = align_up(64 * n, 256);
-  const size_t bp = align_up(4 * (size_t)(n_scenes + 1), 256);
-  cudaError_t e = cudaMalloc(&s->part_arena, 4 * b4 + 5 * bu + bs + 256 + bp + 2 * sizeof(StatsPartial) * kStatsBlocks + 256);
+  const size_t bp = align_up(4 * (size_t)(n_scenes + 1), 256), bi = align_up(8 * (size_t)n_scenes, 256);
+  cudaError_t e = cudaMalloc(&s->part_arena,
+                             4 * b4 + 5 * bu + bs + 256 + bp + bi + 2 * sizeof(StatsPartial) * kStatsBlocks + 256);
   if (e != cudaSuccess) {
     delete s;
     return fail(e == cudaErrorMemoryAllocation ? PS_ERR_NOMEM : PS_ERR_CUDA, std::string("ps_create: ") + cudaGetErrorString(e));
@@ -1180,6 +1207,7 @@ extern "C" int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t 
   s->staging = reinterpret_cast<double*>(p); p += bs;
   s->err = reinterpret_cast<uint32_t*>(p); p += 256;
   s->d_pbase = reinterpret_cast<uint32_t*>(p); p += bp;
+  s->d_interval = reinterpret_cast<double*>(p); p += bi;
   s->d_stats = reinterpret_cast<StatsPartial*>(p); p += sizeof(StatsPartial) * kStatsBlocks;
   s->d_stats_out = reinterpret_cast<StatsPartial*>(p);
   std::vector<uint32_t> pb(n_scenes + 1);
@@ -1201,18 +1229,30 @@ extern "C" int ps_set_state(ps_sim* s, const double* aos, int64_t n_total) {
   if (n_total != s->n_total)
     return fail(PS_ERR_INVALID, "ps_set_state: expected " + std::to_string(s->n_total) + " particles, got " + std::to_string(n_total));
   DeviceGuard guard(s->device);
-  if (!s->grid_sized) {
+  const bool first = !s->grid_sized;
+  if (first) {
     const int rc = size_grids(s, aos);
     if (rc != PS_OK) return rc;
-  } else {
-    for (int sc = 0; sc < s->n_scenes; ++sc)
-      for (int64_t i = s->pbase[sc]; i < s->pbase[sc + 1]; ++i)
-        if (!(2.0 * aos[8 * i + 6] <= s->grids[sc].interval) || !(aos[8 * i + 7] > 0.0))
-          return fail(PS_ERR_INVALID, "ps_set_state: particle " + std::to_string(i) + " does not fit the grid sized by the first upload");
   }
   if (n_total == 0) return PS_OK;
   PS_CUDA(cudaMemcpyAsync(s->staging, aos, 64 * (size_t)n_total, cudaMemcpyHostToDevice, s->stream));
   const unsigned g = blocks_for(n_total);
+  if (!first) {
+    // a later state must fit the grid the first one sized; checked on the
+    // device (a host loop over the records cost milliseconds per upload at
+    // 1M particles), before the state is replaced
+    uint32_t* bad = s->err + 8;
+    uint32_t h_bad = 0;
+    PS_CUDA(cudaMemsetAsync(bad, 0xff, sizeof(uint32_t), s->stream));
+    k_upload_check<<<g, STEP_THREADS, 0, s->stream>>>(s->staging, s->d_pbase, s->n_scenes, s->d_interval, bad,
+                                                        (uint32_t)n_total);
+    PS_CUDA(cudaGetLastError());
+    PS_CUDA(cudaMemcpyAsync(&h_bad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+    PS_CUDA(cudaStreamSynchronize(s->stream));
+    if (h_bad != 0xffffffffu)
+      return fail(PS_ERR_INVALID,
+                  "ps_set_state: particle " + std::to_string(h_bad) + " does not fit the grid sized by the first upload");
+  }
   if (s->precision == PS_FP32)
     k_upload<float><<<g, STEP_THREADS, 0, s->stream>>>(s->staging, static_cast<float4*>(s->P0),
                                                        static_cast<float4*>(s->V1), s->orig, (uint32_t)n_total);

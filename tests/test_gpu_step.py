@@ -178,3 +178,27 @@ def test_bad_inputs_are_errors(need_gpu):
             sim.set_state(bad)
     with pytest.raises(psb200.PSError):
         psb200.Simulation(sc.copy(interval=1e-4), "f32").set_state()  # cell smaller than 2 r_max
+
+
+def test_later_uploads_are_checked_on_the_device(need_gpu):
+    # after the first upload sizes the grids, a new state is checked on the
+    # device: every particle must fit its scene's cell (2 r <= edge) and have
+    # a positive mass; the lowest failing index is reported and the previous
+    # state stays in place
+    batch = [scenes.pile(300, seed=2), scenes.pile(500, seed=3)]
+    with psb200.Simulation(batch, "f64") as sim:
+        sim.set_state()
+        sim.step(5)
+        before = sim.get_state()
+        edge = sim.grid(1).interval
+        for idx, col, val in ((420, 6, 0.51 * edge), (733, 7, 0.0), (301, 6, np.nan), (12, 7, -2.0)):
+            bad = before.copy()
+            bad[idx, col] = val
+            bad[idx + 40, col] = val  # a later failing particle is not the one reported
+            with pytest.raises(psb200.PSError, match=f"particle {idx} does not fit"):
+                sim.set_state(bad)
+            assert np.array_equal(sim.get_state(), before)
+        ok = before.copy()
+        ok[420, 6] = 0.5 * edge  # exactly fits
+        sim.set_state(ok)
+        assert np.array_equal(sim.get_state(), ok)
