@@ -269,25 +269,42 @@ __global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __rest
 template <class T, bool COH>
 __device__ __forceinline__ void rank_move_block(uint32_t blk, const StepBufs<T>& b) {
   const uint32_t base = blk * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
-  uint32_t c[MOVE_PER_THREAD], sl[MOVE_PER_THREAD];
+  // Loads in three dependent rounds, each issued for all MOVE_PER_THREAD
+  // particles before any store (the stores could alias them as far as the
+  // compiler knows, which would otherwise serialise the rounds per particle):
+  // cell, slot and the moved state; the cell's range; the member's orig id.
+  uint32_t c[MOVE_PER_THREAD], sl[MOVE_PER_THREAD], start[MOVE_PER_THREAD], end[MOVE_PER_THREAD],
+      o[MOVE_PER_THREAD];
+  vec4_t<T> P[MOVE_PER_THREAD], V[MOVE_PER_THREAD];
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     const uint32_t p = base + k * STEP_THREADS;
-    c[k] = p < b.n ? b.cell[p] : 0u;
-    sl[k] = p < b.n ? b.slot[p] : 0u;
+    const bool in = p < b.n;
+    c[k] = in ? b.cell[p] : 0u;
+    sl[k] = in ? b.slot[p] : 0u;
+    if (in) {
+      P[k] = b.P1[p];
+      V[k] = b.V1[p];
+    }
   }
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
-    const uint32_t p = base + k * STEP_THREADS;
-    if (p >= b.n) continue;
-    const uint32_t start = ld_ro<COH>(b.offset + c[k]), end = ld_ro<COH>(b.offset + c[k] + 1);
-    const uint32_t o = b.tmp[start + sl[k]];
+    const bool in = base + k * STEP_THREADS < b.n;
+    start[k] = in ? ld_ro<COH>(b.offset + c[k]) : 0u;
+    end[k] = in ? ld_ro<COH>(b.offset + c[k] + 1) : 0u;
+  }
+#pragma unroll
+  for (int k = 0; k < MOVE_PER_THREAD; ++k)
+    o[k] = base + k * STEP_THREADS < b.n ? b.tmp[start[k] + sl[k]] : 0u;
+#pragma unroll
+  for (int k = 0; k < MOVE_PER_THREAD; ++k) {
+    if (base + k * STEP_THREADS >= b.n) continue;
     uint32_t rank = 0;
-    for (uint32_t s = start; s < end; ++s) rank += (b.tmp[s] < o) ? 1u : 0u;
-    const uint32_t d = start + rank;
-    b.P0[d] = b.P1[p];
-    b.V0[d] = b.V1[p];
-    b.orig[d] = o;
+    for (uint32_t s = start[k]; s < end[k]; ++s) rank += (b.tmp[s] < o[k]) ? 1u : 0u;
+    const uint32_t d = start[k] + rank;
+    b.P0[d] = P[k];
+    b.V0[d] = V[k];
+    b.orig[d] = o[k];
     b.scell[d] = c[k];
   }
 }

@@ -223,3 +223,14 @@ def test_adjoint_after_a_forward_on_lists(need_gpu, prec):
             out[skin] = (final, grads[0], g0)
     assert same(out[0.05][0], out[None][0])
     assert np.array_equal(out[0.05][1], out[None][1]) and np.array_equal(out[0.05][2], out[None][2])
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_lists_batch_with_empty_and_single_sphere_scenes(need_gpu, prec):
+    one = scenes.pile(1, seed=25)
+    empty = one.copy(state=np.zeros((0, 8)))
+    batch = [scenes.pile(400, seed=26, k_spring=1.0), empty, one, scenes.pile(200, seed=27, k_spring=1.0), empty]
+    want, _ = run(batch, prec, calls=(1, 50, 30))
+    got, (_, fb) = run(batch, prec, calls=(1, 50, 30), skin=0.05)
+    assert fb == 0
+    assert same(got, want)
