@@ -133,19 +133,25 @@ extern "C" void runSimulateCUDA(const std::vector<psb_compat::ParticlePtr>& part
                        std::to_string(g.nb[2]) + ")");
   log_line("info", "# interval                          : " + d2s(g.interval));
   log_line("info", "# precision                         : " + std::string(precision == PS_FP32 ? "fp32" : "fp64"));
-  // neighbour lists (same results as the grid path): "auto" tunes the skin,
-  // a number sets it (0 keeps the grid path)
+  // neighbour lists (same results as the grid path): "auto" tunes the skin
+  // (about 1,000 trial steps, so only for runs of 10,000 steps or more; a
+  // shorter run keeps the grid path), a number sets it (0 keeps the grid path)
   if (const char* nl = std::getenv("PSB200_NEIGHBOR_LISTS")) {
-    double skin = 0.0;
-    if (std::string(nl) == "auto") {
-      const double skins[] = {0.0, 0.02, 0.05, 0.1, 0.2};
-      double ms[5];
-      check(ps_tune_neighbor_lists(sim, 100, skins, 5, 64, ms, &skin), "tuning neighbour lists");
+    const std::string mode(nl);
+    if (mode == "auto" && maxSteps < 10000) {
+      log_line("info", "# neighbour lists (auto)            : off for runs under 10,000 steps");
     } else {
-      skin = std::atof(nl);
-      check(ps_set_neighbor_lists(sim, skin, 64), "neighbour lists");
+      double skin = 0.0;
+      if (mode == "auto") {
+        const double skins[] = {0.0, 0.02, 0.05, 0.1, 0.2};
+        double ms[5];
+        check(ps_tune_neighbor_lists(sim, 100, skins, 5, 64, ms, &skin), "tuning neighbour lists");
+      } else {
+        skin = std::atof(nl);
+        check(ps_set_neighbor_lists(sim, skin, 64), "neighbour lists");
+      }
+      log_line("info", "# neighbour-list skin (x cell edge) : " + d2s(skin));
     }
-    log_line("info", "# neighbour-list skin (x cell edge) : " + d2s(skin));
   }
   log_line("info", "##############################################################################################################");
 

@@ -174,10 +174,11 @@ def test_list_arguments(need_gpu):
         assert sim.list_stats_all() == (0, 0, 0)
 
 
-@pytest.mark.parametrize("setting", ["auto", "0.05"])
-def test_cli_with_neighbor_lists_writes_the_same_csv(need_gpu, tmp_path, setting):
+@pytest.mark.parametrize("setting,steps", [("auto", 10000), ("auto", 400), ("0.05", 400)])
+def test_cli_with_neighbor_lists_writes_the_same_csv(need_gpu, tmp_path, setting, steps):
     """runSimulateCUDA with PSB200_NEIGHBOR_LISTS: the output CSV is the
-    grid path's, byte for byte."""
+    grid path's, byte for byte.  "auto" tunes only for runs of 10,000 steps
+    or more; a shorter run keeps the grid path and says so."""
     sc = scenes.pile(2000, seed=23, k_spring=1.0)
     csv_in = tmp_path / "in.csv"
     with open(csv_in, "w") as f:
@@ -187,7 +188,7 @@ def test_cli_with_neighbor_lists_writes_the_same_csv(need_gpu, tmp_path, setting
     outs = {}
     for tag, env_value in (("grid", None), ("lists", setting)):
         out = tmp_path / f"{tag}.csv"
-        cmd = [psb200.CLI_PATH, "--lib", psb200.LIB_PATH, str(csv_in), "--cuda", "--max-steps", "400",
+        cmd = [psb200.CLI_PATH, "--lib", psb200.LIB_PATH, str(csv_in), "--cuda", "--max-steps", str(steps),
                "--box-min", *map(str, sc.box_min), "--box-max", *map(str, sc.box_max), "--dt", "1e-05",
                "--coeff-of-spring", "1", "--coeff-of-restitution-sphere", "0.5",
                "--coeff-of-restitution-wall", *["0.7"] * 6, "--gravity", "0", "0", "-9.8",
@@ -198,7 +199,9 @@ def test_cli_with_neighbor_lists_writes_the_same_csv(need_gpu, tmp_path, setting
             env["PSB200_NEIGHBOR_LISTS"] = env_value
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
         assert r.returncode == 0, r.stdout + r.stderr
-        if env_value is not None:
+        if env_value == "auto" and steps < 10000:
+            assert "off for runs under 10,000 steps" in r.stdout
+        elif env_value is not None:
             assert "neighbour-list skin" in r.stdout
         outs[tag] = out.read_text()
     assert outs["lists"] == outs["grid"]
