@@ -237,3 +237,23 @@ def test_lists_batch_with_empty_and_single_sphere_scenes(need_gpu, prec):
     got, (_, fb) = run(batch, prec, calls=(1, 50, 30), skin=0.05)
     assert fb == 0
     assert same(got, want)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_lists_over_a_40000_step_settling_run(need_gpu, prec):
+    # the lattice collapses into a pile and comes close to rest: thousands of
+    # contacts change order and lists are rebuilt many times; the end state
+    # must still be the grid path's bit for bit
+    sc = scenes.settle_pile(side=16)
+    calls = (10000,) * 4
+    want, _ = run(sc, prec, calls=calls)
+    with psb200.Simulation(sc, prec) as sim:
+        sim.set_state()
+        sim.set_neighbor_lists(0.05, 64)
+        for n in calls:
+            sim.step(n)
+        got = sim.get_state()
+        rebuilds, fallbacks, grid_steps = sim.list_stats_all()
+    print(f"\nsettling pile {prec}: {rebuilds} rebuilds, {fallbacks} fallbacks, {grid_steps} steps on the grid path")
+    assert rebuilds > 10
+    assert same(got, want)
