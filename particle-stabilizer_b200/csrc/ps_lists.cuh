@@ -103,21 +103,39 @@ __device__ __forceinline__ void list_build_one(uint32_t i, const StepBufs<T>& b,
     axis_span<T>(P.y, reach, sp.grid_lo[1], sp.interval, sp.nb[1], y0, y1);
     axis_span<T>(P.z, reach, sp.grid_lo[2], sp.interval, sp.nb[2], z0, z1);
     const uint32_t ny = (uint32_t)sp.nb[1], nz = (uint32_t)sp.nb[2];
-    for (int32_t bx = x0; bx <= x1; ++bx) {
-      for (int32_t by = y0; by <= y1; ++by) {
-        const uint32_t col = sp.cbase + ((uint32_t)bx * ny + (uint32_t)by) * nz;
-        const uint32_t j0 = ld_ro<COH>(b.offset + col + (uint32_t)z0);
-        const uint32_t j1 = ld_ro<COH>(b.offset + col + (uint32_t)z1 + 1u);
-        for (uint32_t j = j0; j < j1; ++j) {
-          if (j == i) continue;
-          const vec4_t<T> Q = ld4c<T, COH>(b.P0 + j);
-          const T dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
-          // generous cut-off: the list may hold more than needed, never less
-          const T cut = (P.w + Q.w + skin) * T(1.0001);
-          if (dx * dx + dy * dy + dz * dz < cut * cut) {
-            if (k < L.cap) L.list[(size_t)k * b.n + i] = j;
-            ++k;
-          }
+    // candidates of one column's slot range [j0, j1)
+    auto walk = [&](uint32_t j0, uint32_t j1) {
+      for (uint32_t j = j0; j < j1; ++j) {
+        if (j == i) continue;
+        const vec4_t<T> Q = ld4c<T, COH>(b.P0 + j);
+        const T dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
+        // generous cut-off: the list may hold more than needed, never less
+        const T cut = (P.w + Q.w + skin) * T(1.0001);
+        if (dx * dx + dy * dy + dz * dz < cut * cut) {
+          if (k < L.cap) L.list[(size_t)k * b.n + i] = j;
+          ++k;
+        }
+      }
+    };
+    if (x1 - x0 < 3 && y1 - y0 < 3) {
+      // the usual span of at most 3 x 3 columns: all range bounds are loaded
+      // before the walk, which visits the columns in the same order
+      uint32_t lo[9], hi[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        const int32_t bx = x0 + q / 3, by = y0 + q % 3;
+        const bool ok = bx <= x1 && by <= y1;
+        const uint32_t col = sp.cbase + ((uint32_t)(ok ? bx : x0) * ny + (uint32_t)(ok ? by : y0)) * nz;
+        lo[q] = ok ? ld_ro<COH>(b.offset + col + (uint32_t)z0) : 0u;
+        hi[q] = ok ? ld_ro<COH>(b.offset + col + (uint32_t)z1 + 1u) : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < 9; ++q) walk(lo[q], hi[q]);
+    } else {
+      for (int32_t bx = x0; bx <= x1; ++bx) {
+        for (int32_t by = y0; by <= y1; ++by) {
+          const uint32_t col = sp.cbase + ((uint32_t)bx * ny + (uint32_t)by) * nz;
+          walk(ld_ro<COH>(b.offset + col + (uint32_t)z0), ld_ro<COH>(b.offset + col + (uint32_t)z1 + 1u));
         }
       }
     }
