@@ -1020,8 +1020,9 @@ size_t tape_row_bytes(size_t vec_bytes, int64_t n) {
 }
 
 // Recompute `steps` steps of a block eagerly (box containers): step k's
-// contact kernel writes tape row k + 1 and its cell offsets are copied to
-// offsets slot k.
+// contact kernel writes tape row k + 1, and its scan writes the cell offsets
+// straight into offsets slot k, which its scatter, rank/move and contacts
+// then read (no copy of the offsets per step).
 template <class T, bool MULTI>
 int enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes, uint32_t* offs, size_t offs_stride) {
   StepBufs<T> b = bufs<T>(s);
@@ -1035,16 +1036,16 @@ int enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes, 
     b.tape_p = row.p;
     b.tape_v = row.v;
     b.tape_o = row.o;
-    pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, n_scan(s),
+    uint32_t* off_k = offs + offs_stride * (size_t)k;
+    b.offset = off_k;
+    pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, off_k, n_scan(s),
                (const uint32_t*)s->tile_sum);
     pdl_launch(k_scatter, move_blocks(s->n_total, b.n_tiles), STEP_THREADS, st, (const uint32_t*)s->cell, s->slot,
-               (const uint32_t*)s->orig, (const uint32_t*)s->offset, s->tmp, s->count, (uint32_t)s->n_total,
+               (const uint32_t*)s->orig, (const uint32_t*)off_k, s->tmp, s->count, (uint32_t)s->n_total,
                s->tile_sum, b.n_tiles);
     pdl_launch(k_rank_move<T>, move_blocks(s->n_total, 0), STEP_THREADS, st, b);
     b.tape_vpre = row.vpre;
     b.tape_cell = row.cell;
-    PS_CUDA(cudaMemcpyAsync(offs + offs_stride * (size_t)k, s->offset, sizeof(uint32_t) * (size_t)n_scan(s),
-                            cudaMemcpyDeviceToDevice, st));
     const MeshView* mv = s->d_mesh_view;
     if (k + 1 < steps)
       pdl_launch(k_contacts<T, MULTI, false, true>, gp, STEP_THREADS, st, b, sp0, mv);
