@@ -140,6 +140,7 @@ struct ps_sim {
   // LIST_BACKOFF_RATE steps sends the next `list_backoff` steps to the grid path
   int64_t list_win_steps = 0, list_win_rebuilds = 0, list_backoff = 0, list_backoff_len = 0;
   unsigned list_rebuild_grid = 0;         // CTAs of the cooperative rebuild (one wave)
+  unsigned list_step_grid = 0;            // CTAs of the list step kernel (one wave)
 };
 
 namespace {
@@ -375,22 +376,28 @@ cudaError_t enqueue_steps_list(ps_sim* s, int64_t steps) {
                                                (uint32_t)gm0, (uint32_t)gm1);
       if (e != cudaSuccess) return e;
     }
+    const unsigned gl = std::min(gp, s->list_step_grid);
     if (k + 1 < steps)
-      pdl_launch(k_contacts_list<T, MULTI, MESH, true>, gp, STEP_THREADS, st, b, sp0, mv, L, par);
+      pdl_launch(k_contacts_list<T, MULTI, MESH, true>, gl, STEP_THREADS, st, b, sp0, mv, L, par);
     else
-      pdl_launch(k_contacts_list<T, MULTI, MESH, false>, gp, STEP_THREADS, st, b, sp0, mv, L, par);
+      pdl_launch(k_contacts_list<T, MULTI, MESH, false>, gl, STEP_THREADS, st, b, sp0, mv, L, par);
   }
   return cudaGetLastError();
 }
 
-// CTAs of one wave of k_list_rebuild, which its grid barriers need resident.
-template <class T, bool MULTI>
-int rebuild_grid(ps_sim* s, unsigned& grid) {
-  int per_sm = 0, sms = 0;
+// CTAs of one wave of k_list_rebuild, which its grid barriers need resident,
+// and of one wave of the list step kernel, which loops over the spheres.
+template <class T, bool MULTI, bool MESH>
+int list_grids(ps_sim* s) {
+  int per_sm = 0, step_per_sm = 0, sms = 0;
   PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_list_rebuild<T, MULTI>, STEP_THREADS, 0));
+  PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&step_per_sm, k_contacts_list<T, MULTI, MESH, true>,
+                                                        STEP_THREADS, 0));
   PS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
-  if (per_sm < 1 || sms < 1) return fail(PS_ERR_CUDA, "ps_step: the list rebuild kernel cannot be resident");
-  grid = (unsigned)(per_sm * sms);
+  if (per_sm < 1 || step_per_sm < 1 || sms < 1)
+    return fail(PS_ERR_CUDA, "ps_step: the list kernels cannot be resident");
+  s->list_rebuild_grid = (unsigned)(per_sm * sms);
+  s->list_step_grid = (unsigned)(step_per_sm * sms);
   return PS_OK;
 }
 
@@ -1352,11 +1359,13 @@ int step_lists(ps_sim* s, int64_t n_steps) {
     s->list_bytes = need;
   }
   if (s->list_rebuild_grid == 0) {
-    const int g = s->precision == PS_FP32
-                      ? (s->multi ? rebuild_grid<float, true>(s, s->list_rebuild_grid)
-                                  : rebuild_grid<float, false>(s, s->list_rebuild_grid))
-                      : (s->multi ? rebuild_grid<double, true>(s, s->list_rebuild_grid)
-                                  : rebuild_grid<double, false>(s, s->list_rebuild_grid));
+    int g;
+    if (s->precision == PS_FP32)
+      g = s->multi ? (s->has_mesh ? list_grids<float, true, true>(s) : list_grids<float, true, false>(s))
+                   : (s->has_mesh ? list_grids<float, false, true>(s) : list_grids<float, false, false>(s));
+    else
+      g = s->multi ? (s->has_mesh ? list_grids<double, true, true>(s) : list_grids<double, true, false>(s))
+                   : (s->has_mesh ? list_grids<double, false, true>(s) : list_grids<double, false, false>(s));
     if (g != PS_OK) return g;
   }
   uint32_t* rebuilds = s->precision == PS_FP32 ? list_bufs<float>(s).flag + LIST_REBUILDS
