@@ -111,89 +111,90 @@ __device__ __forceinline__ bool pair_active(const vec4_t<T>& P, const vec4_t<T>&
 
 template <class T, bool MULTI>
 __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, AdjBufs<T> a, SceneParams<T> sp0) {
-  const uint32_t i = blockIdx.x * STEP_THREADS + threadIdx.x;
-  if (i >= b.n) return;
-  const SceneParams<T>& sp = scene_of<T, MULTI>(i, sp0, b.scenes, b.pbase, b.n_scenes);
-  const vec4_t<T> P = b.P0[i];
-  const vec4_t<T> V = b.V0[i];
-  const uint32_t oi = b.orig[i];
-  a.inv[oi] = i;
-  const vec4_t<T> G = a.av[i], X = a.ax[i];
-  const T gx = G.x, gy = G.y, gz = G.z;
-  T xb0 = X.x, xb1 = X.y, xb2 = X.z;
-  T vb0 = gx, vb1 = gy, vb2 = gz;
-  double dk = 0.0, de = 0.0;
-  int32_t cx, cy, cz;
-  cell_coords<T>(b.scell[i], sp, cx, cy, cz);
-  const int32_t nx = sp.nb[0], ny = sp.nb[1], nz = sp.nb[2];
-  const uint32_t z0 = (uint32_t)(cz > 0 ? cz - 1 : 0);
-  const uint32_t z1 = (uint32_t)(cz + 1 < nz ? cz + 1 : nz - 1) + 1u;
-  const T k = sp.k_spring, e = sp.e_sphere;
-  const bool live = isfinite(P.x) && isfinite(P.y) && isfinite(P.z);  // no active pair otherwise
-  uint32_t lo[9], hi[9];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) {  // the 18 range bounds, loaded together
-    const int32_t bx = cx - 1 + q / 3, by = cy - 1 + q % 3;
-    const bool ok = live && bx >= 0 && bx < nx && by >= 0 && by < ny;
-    const uint32_t col = ok ? sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz : sp.cbase;
-    lo[q] = ok ? __ldg(b.offset + col + z0) : 0u;
-    hi[q] = ok ? __ldg(b.offset + col + z1) : 0u;
-  }
-#pragma unroll
-  for (int q = 0; q < 9; ++q)
-    for (uint32_t j = lo[q]; j < hi[q]; ++j) {
-      if (j == i) continue;
-      const vec4_t<T> Pj = ld4<T>(b.P0 + j);
-      if (!pair_active<T>(P, Pj)) continue;
-      const vec4_t<T> Vj = b.V0[j];
-      const vec4_t<T> H = a.av[j];
-      PairGeom<T> g;
-      g.dx = P.x - Pj.x;
-      g.dy = P.y - Pj.y;
-      g.dz = P.z - Pj.z;
-      g.ux = V.x - Vj.x;
-      g.uy = V.y - Vj.y;
-      g.uz = V.z - Vj.z;
-      g.R = P.w + Pj.w;
-      const T L2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz;
-      g.L = sqrt(L2);
-      g.iL = T(1) / g.L;
-      g.iL2 = T(1) / L2;
-      g.ov = g.R - g.L;
-      g.ud = g.ux * g.dx + g.uy * g.dy + g.uz * g.dz;
-      const T inv_msum = T(1) / (V.w + Vj.w);
-      T ddx, ddy, ddz, dux, duy, duz;
-      // i receives from j
-      pair_adjoint<T>(g, T(1), V.w, Vj.w, inv_msum, k, e, gx, gy, gz, ddx, ddy, ddz, dux, duy, duz, dk, de);
-      xb0 += ddx;
-      xb1 += ddy;
-      xb2 += ddz;
-      vb0 += dux;
-      vb1 += duy;
-      vb2 += duz;
-      // j receives from i: that direction's d and u are -d and -u, so its
-      // adjoints with respect to the stored d and u come back sign-mapped;
-      // its parameter partials belong to j's own thread
-      double dk2 = 0.0, de2 = 0.0;
-      pair_adjoint<T>(g, T(-1), Vj.w, V.w, inv_msum, k, e, H.x, H.y, H.z, ddx, ddy, ddz, dux, duy, duz, dk2, de2);
-      xb0 += ddx;
-      xb1 += ddy;
-      xb2 += ddz;
-      vb0 += dux;
-      vb1 += duy;
-      vb2 += duz;
+  // one wave of CTAs (occupancy x SMs, the host's choice) loops over the particles
+  for (uint32_t i = blockIdx.x * STEP_THREADS + threadIdx.x; i < b.n; i += gridDim.x * STEP_THREADS) {
+    const SceneParams<T>& sp = scene_of<T, MULTI>(i, sp0, b.scenes, b.pbase, b.n_scenes);
+    const vec4_t<T> P = b.P0[i];
+    const vec4_t<T> V = b.V0[i];
+    const uint32_t oi = b.orig[i];
+    a.inv[oi] = i;
+    const vec4_t<T> G = a.av[i], X = a.ax[i];
+    const T gx = G.x, gy = G.y, gz = G.z;
+    T xb0 = X.x, xb1 = X.y, xb2 = X.z;
+    T vb0 = gx, vb1 = gy, vb2 = gz;
+    double dk = 0.0, de = 0.0;
+    int32_t cx, cy, cz;
+    cell_coords<T>(b.scell[i], sp, cx, cy, cz);
+    const int32_t nx = sp.nb[0], ny = sp.nb[1], nz = sp.nb[2];
+    const uint32_t z0 = (uint32_t)(cz > 0 ? cz - 1 : 0);
+    const uint32_t z1 = (uint32_t)(cz + 1 < nz ? cz + 1 : nz - 1) + 1u;
+    const T k = sp.k_spring, e = sp.e_sphere;
+    const bool live = isfinite(P.x) && isfinite(P.y) && isfinite(P.z);  // no active pair otherwise
+    uint32_t lo[9], hi[9];
+  #pragma unroll
+    for (int q = 0; q < 9; ++q) {  // the 18 range bounds, loaded together
+      const int32_t bx = cx - 1 + q / 3, by = cy - 1 + q % 3;
+      const bool ok = live && bx >= 0 && bx < nx && by >= 0 && by < ny;
+      const uint32_t col = ok ? sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz : sp.cbase;
+      lo[q] = ok ? __ldg(b.offset + col + z0) : 0u;
+      hi[q] = ok ? __ldg(b.offset + col + z1) : 0u;
     }
-  vec4_t<T> xo = X, vo = G;
-  xo.x = xb0;
-  xo.y = xb1;
-  xo.z = xb2;
-  vo.x = vb0;
-  vo.y = vb1;
-  vo.z = vb2;
-  a.ax2[i] = xo;
-  a.av2[i] = vo;
-  a.acc[(size_t)ADJ_K * a.n + i] += dk;
-  a.acc[(size_t)ADJ_E * a.n + i] += de;
+  #pragma unroll
+    for (int q = 0; q < 9; ++q)
+      for (uint32_t j = lo[q]; j < hi[q]; ++j) {
+        if (j == i) continue;
+        const vec4_t<T> Pj = ld4<T>(b.P0 + j);
+        if (!pair_active<T>(P, Pj)) continue;
+        const vec4_t<T> Vj = b.V0[j];
+        const vec4_t<T> H = a.av[j];
+        PairGeom<T> g;
+        g.dx = P.x - Pj.x;
+        g.dy = P.y - Pj.y;
+        g.dz = P.z - Pj.z;
+        g.ux = V.x - Vj.x;
+        g.uy = V.y - Vj.y;
+        g.uz = V.z - Vj.z;
+        g.R = P.w + Pj.w;
+        const T L2 = g.dx * g.dx + g.dy * g.dy + g.dz * g.dz;
+        g.L = sqrt(L2);
+        g.iL = T(1) / g.L;
+        g.iL2 = T(1) / L2;
+        g.ov = g.R - g.L;
+        g.ud = g.ux * g.dx + g.uy * g.dy + g.uz * g.dz;
+        const T inv_msum = T(1) / (V.w + Vj.w);
+        T ddx, ddy, ddz, dux, duy, duz;
+        // i receives from j
+        pair_adjoint<T>(g, T(1), V.w, Vj.w, inv_msum, k, e, gx, gy, gz, ddx, ddy, ddz, dux, duy, duz, dk, de);
+        xb0 += ddx;
+        xb1 += ddy;
+        xb2 += ddz;
+        vb0 += dux;
+        vb1 += duy;
+        vb2 += duz;
+        // j receives from i: that direction's d and u are -d and -u, so its
+        // adjoints with respect to the stored d and u come back sign-mapped;
+        // its parameter partials belong to j's own thread
+        double dk2 = 0.0, de2 = 0.0;
+        pair_adjoint<T>(g, T(-1), Vj.w, V.w, inv_msum, k, e, H.x, H.y, H.z, ddx, ddy, ddz, dux, duy, duz, dk2, de2);
+        xb0 += ddx;
+        xb1 += ddy;
+        xb2 += ddz;
+        vb0 += dux;
+        vb1 += duy;
+        vb2 += duz;
+      }
+    vec4_t<T> xo = X, vo = G;
+    xo.x = xb0;
+    xo.y = xb1;
+    xo.z = xb2;
+    vo.x = vb0;
+    vo.y = vb1;
+    vo.z = vb2;
+    a.ax2[i] = xo;
+    a.av2[i] = vo;
+    a.acc[(size_t)ADJ_K * a.n + i] += dk;
+    a.acc[(size_t)ADJ_E * a.n + i] += de;
+  }
 }
 
 // Walls + integrate adjoint over the tape row's sorted slots.  The step

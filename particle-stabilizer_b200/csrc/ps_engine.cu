@@ -1123,6 +1123,14 @@ int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl
   double* red = reinterpret_cast<double*>(p);
   cudaStream_t st = s->stream;
   const unsigned gp = blocks_for(n);
+  unsigned adj_grid = 0;  // one wave of k_adj_contacts, which loops over the particles
+  {
+    int per_sm = 0, sms = 0;
+    PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_contacts<T, MULTI>, STEP_THREADS, 0));
+    PS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    if (per_sm < 1 || sms < 1) return fail(PS_ERR_CUDA, "ps_backward: the adjoint contact kernel cannot be resident");
+    adj_grid = (unsigned)(per_sm * sms);
+  }
   // the final state's order (recomputing the last block reproduces it exactly)
   int rc0 = load_state(s, s->fwd_ckpt.back());
   if (rc0 != PS_OK) return rc0;
@@ -1150,7 +1158,7 @@ int backward_impl(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl
       b.scell = g.cell;
       b.offset = offs + offs_stride * (size_t)t;
       a.tape = tape_row<T>(tape, row_b, n, t);
-      k_adj_contacts<T, MULTI><<<gp, STEP_THREADS, 0, st>>>(b, a, sp0);
+      k_adj_contacts<T, MULTI><<<std::min(gp, adj_grid), STEP_THREADS, 0, st>>>(b, a, sp0);
       k_adj_walls_integrate<T, MULTI><<<gp, STEP_THREADS, 0, st>>>(b, a, sp0);
       PS_CUDA(cudaGetLastError());
     }
