@@ -141,7 +141,6 @@ struct ps_sim {
   int64_t list_win_steps = 0, list_win_rebuilds = 0, list_backoff = 0, list_backoff_len = 0;
   unsigned list_rebuild_grid = 0;         // CTAs of the cooperative rebuild (one wave)
   unsigned list_step_grid = 0;            // CTAs of the list step kernel (one wave)
-  unsigned contacts_grid = 0;             // CTAs of k_contacts (one wave), set with the grids
 };
 
 namespace {
@@ -237,9 +236,9 @@ int64_t enqueue_steps(ps_sim* s, int64_t steps) {
                (const uint32_t*)s->orig, (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles);
     pdl_launch(k_rank_move<T>, move_blocks(s->n_total, 0), STEP_THREADS, st, b);
     if (k + 1 < steps)
-      pdl_launch(k_contacts<T, MULTI, MESH, true>, std::min(gp, s->contacts_grid), STEP_THREADS, st, b, sp0, mv);
+      pdl_launch(k_contacts<T, MULTI, MESH, true>, gp, STEP_THREADS, st, b, sp0, mv);
     else
-      pdl_launch(k_contacts<T, MULTI, MESH, false>, std::min(gp, s->contacts_grid), STEP_THREADS, st, b, sp0, mv);
+      pdl_launch(k_contacts<T, MULTI, MESH, false>, gp, STEP_THREADS, st, b, sp0, mv);
     launches += 4;
   }
   return launches;
@@ -281,9 +280,9 @@ void enqueue_steps_recorded(ps_sim* s, int64_t steps, std::vector<LaunchRecord>&
     post();
     pre(PS_K_CONTACTS);
     if (k + 1 < steps)
-      k_contacts<T, MULTI, MESH, true><<<std::min(gp, s->contacts_grid), STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+      k_contacts<T, MULTI, MESH, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
     else
-      k_contacts<T, MULTI, MESH, false><<<std::min(gp, s->contacts_grid), STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+      k_contacts<T, MULTI, MESH, false><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
     post();
   }
 }
@@ -793,18 +792,6 @@ void apply_l2_window(ps_sim* s, cudaGraph_t g, bool clear = false) {
   cudaGetLastError();
 }
 
-// CTAs of one wave of k_contacts (the fused variant, the largest), which
-// loops over the particles.
-template <class T, bool MULTI, bool MESH>
-int set_contacts_grid(ps_sim* s) {
-  int per_sm = 0, sms = 0;
-  PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contacts<T, MULTI, MESH, true>, STEP_THREADS, 0));
-  PS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
-  if (per_sm < 1 || sms < 1) return fail(PS_ERR_CUDA, "the contact kernel cannot be resident");
-  s->contacts_grid = (unsigned)(per_sm * sms);
-  return PS_OK;
-}
-
 // Size every scene's grid from its radii and allocate the per-cell arrays.
 int size_grids(ps_sim* s, const double* aos) {
   s->grids.assign(s->n_scenes, GridHost{});
@@ -922,16 +909,6 @@ int size_grids(ps_sim* s, const double* aos) {
   }
   {
     const int rc = s->precision == PS_FP32 ? upload_bounds<float>(s) : upload_bounds<double>(s);
-    if (rc != PS_OK) return rc;
-  }
-  if (s->contacts_grid == 0) {
-    int rc;
-    if (s->precision == PS_FP32)
-      rc = s->multi ? (s->has_mesh ? set_contacts_grid<float, true, true>(s) : set_contacts_grid<float, true, false>(s))
-                    : (s->has_mesh ? set_contacts_grid<float, false, true>(s) : set_contacts_grid<float, false, false>(s));
-    else
-      rc = s->multi ? (s->has_mesh ? set_contacts_grid<double, true, true>(s) : set_contacts_grid<double, true, false>(s))
-                    : (s->has_mesh ? set_contacts_grid<double, false, true>(s) : set_contacts_grid<double, false, false>(s));
     if (rc != PS_OK) return rc;
   }
   const size_t spb = s->precision == PS_FP32 ? sizeof(SceneParams<float>) : sizeof(SceneParams<double>);
@@ -1078,9 +1055,9 @@ int enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes, 
     b.tape_cell = row.cell;
     const MeshView* mv = s->d_mesh_view;
     if (k + 1 < steps)
-      pdl_launch(k_contacts<T, MULTI, false, true>, std::min(gp, s->contacts_grid), STEP_THREADS, st, b, sp0, mv);
+      pdl_launch(k_contacts<T, MULTI, false, true>, gp, STEP_THREADS, st, b, sp0, mv);
     else
-      pdl_launch(k_contacts<T, MULTI, false, false>, std::min(gp, s->contacts_grid), STEP_THREADS, st, b, sp0, mv);
+      pdl_launch(k_contacts<T, MULTI, false, false>, gp, STEP_THREADS, st, b, sp0, mv);
   }
   return PS_OK;
 }

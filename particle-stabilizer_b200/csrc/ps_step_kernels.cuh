@@ -367,15 +367,10 @@ __device__ __forceinline__ void cell_coords(uint32_t c, const SceneParams<T>& sp
 template <class T, bool MULTI, bool MESH, bool FUSED>
 __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 4 : 3) k_contacts(StepBufs<T> b, SceneParams<T> sp0,
                                                                                   const MeshView* mv) {
-  pdl_wait();
-  // One wave of CTAs (occupancy x SMs, the host's choice) loops over the
-  // particles: no tail wave and no per-CTA start-up (1M spheres FP32: 58.3 ->
-  // 54.8 us).  The loop bound is the same for the whole CTA, so every lane
-  // reaches count_cell's warp collectives.
-  for (uint32_t base = blockIdx.x * STEP_THREADS; base < b.n; base += gridDim.x * STEP_THREADS) {
-  const uint32_t i = base + threadIdx.x;
+  const uint32_t i = blockIdx.x * STEP_THREADS + threadIdx.x;
   const bool valid = i < b.n;
   uint32_t c = 0;
+  pdl_wait();
   if (valid) {
     const SceneParams<T>& sp = scene_of<T, MULTI>(i, sp0, b.scenes, b.pbase, b.n_scenes);
     vec4_t<T> P = b.P0[i];
@@ -440,7 +435,6 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 4 : 3) k_contac
   }
   if (FUSED) {
     count_cell(b.count, b.tile_sum, c, valid);
-  }
   }
 }
 
