@@ -17,16 +17,17 @@
 //
 // Rebuilds.  The step kernel also integrates the next step (as the fused
 // k_contacts) and tests whether some sphere has moved more than about
-// skin / 2 from where the lists were built; warps that see one set a flag
+// skin / 2 from where the lists were built; warps that see one set the flag
 // word of the next step's parity.  Before each step a cooperative kernel,
-// one wave of CTAs, reads that word: clear, it returns at once (about a
-// microsecond; a conditional graph node costs ten); set, it runs count,
-// scan, scatter, rank/move and list build as phases separated by grid
-// barriers.  The step kernel clears the word of its own parity, which that
-// kernel has read, for the step after next.  A list longer than the capacity, or a sphere
-// whose overlapping pairs change order and outnumber the sort buffer, sets
-// PS_DEVERR_LIST_OVERFLOW, and a barrier that waits too long sets
-// PS_DEVERR_LIST_BARRIER; the host then repeats the call on the grid path.
+// one wave of CTAs, reads the word of that step's parity: clear, it returns
+// at once (about a microsecond; a conditional graph node costs ten); set, it
+// runs count, scan, scatter, rank/move and list build as phases separated by
+// grid barriers.  Each step kernel clears its own parity's word, which the
+// rebuild before it has read, for the step after next.  A list longer than
+// the capacity, or a sphere whose overlapping pairs change order and
+// outnumber the sort buffer, sets PS_DEVERR_LIST_OVERFLOW, and a barrier
+// that waits too long sets PS_DEVERR_LIST_BARRIER; the host then repeats
+// the call on the grid path.
 #pragma once
 
 #include "ps_step_kernels.cuh"
