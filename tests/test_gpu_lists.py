@@ -105,14 +105,25 @@ def test_lists_batch(need_gpu):
         assert same(got, want)
 
 
+@pytest.mark.parametrize("prec", ["f32", "f64"])
 @pytest.mark.parametrize("make", [lambda: scenes.box_mesh_scene(), lambda: scenes.funnel_wall_scene(1500)],
                          ids=["box_mesh", "funnel"])
-def test_lists_triangle_containers(need_gpu, make):
+def test_lists_triangle_containers(need_gpu, make, prec):
     sc = make()
-    want, _ = run(sc, "f32", calls=(120, 80))
-    got, (_, fb) = run(sc, "f32", calls=(120, 80), skin=0.3)
+    want, _ = run(sc, prec, calls=(120, 80))
+    got, (_, fb) = run(sc, prec, calls=(120, 80), skin=0.3)
     assert fb == 0
     assert same(got, want)
+
+
+def test_lists_batch_with_a_triangle_container(need_gpu):
+    # a mesh scene and box scenes in one launch (the multi-scene mesh variant)
+    batch = [scenes.pile(300, seed=28, k_spring=1.0), scenes.box_mesh_scene(), scenes.pile(500, seed=29, k_spring=1.0)]
+    for prec in ("f32", "f64"):
+        want, _ = run(batch, prec, calls=(60, 90))
+        got, (_, fb) = run(batch, prec, calls=(60, 90), skin=0.2)
+        assert fb == 0
+        assert same(got, want)
 
 
 def test_list_overflow_repeats_call_on_grid(need_gpu):
