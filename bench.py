@@ -393,6 +393,57 @@ def lists_measure(psb200, scenes_mod, device, only=None, fixed_skin=None) -> dic
     return out
 
 
+def reference_cuda_measure(psb200, scenes_mod, device, steps: int = 200, warm: int = 20) -> dict:
+    """The reference's own CUDA simulator (oracle/_ref/libref_cuda.so, built
+    from its unmodified sources for sm_100a, driven per step) against this
+    library on the same B200, in the same process.
+
+    Scene: the 1M-sphere box scene with spring 0.25 instead of 5e4, all other
+    draws identical.  With the specified spring the scheme diverges, and the
+    reference's count/register kernels index out of range once positions
+    stop being finite, so the reference runs only here, and only after this
+    library's FP64 run of the same steps stayed finite and inside the box.
+    Both time steps warm+1 .. warm+steps from the same initial state (device
+    time, CUDA events)."""
+    from oracle import ps_oracle as O
+
+    if not os.path.exists(O.REF_CUDA_SO):
+        return {"unavailable": "oracle/_ref/libref_cuda.so was not built (reference sources absent at build time)"}
+    sc = scenes_mod.c2_scene(k_spring=0.25)
+    ours = {}
+    for prec in ("f32", "f64"):
+        with psb200.Simulation(sc, prec, device=device) as sim:
+            sim.set_state()
+            sim.step(warm)
+            sim.checkpoint_save(1)
+            sim.time_steps(steps)  # captures the graphs of this block length
+            sim.checkpoint_load(1)
+            ms = sim.time_steps(steps)
+            st = sim.get_state()
+        inside = bool(np.isfinite(st).all() and np.all(st[:, :3] >= np.array(sc.box_min))
+                      and np.all(st[:, :3] <= np.array(sc.box_max)))
+        ours[prec] = {"ms_per_step": ms / steps, "particle_steps_per_s": sc.n * steps / (ms * 1e-3),
+                      "finite_and_inside_box": inside}
+    if not ours["f64"]["finite_and_inside_box"]:
+        return {"unavailable": "this library's FP64 run left the box or went non-finite; reference not run"}
+    r = O.ref_cuda()
+    h = r.create(sc)
+    try:
+        r.step(h, warm)
+        ref_s = r.time_steps(h, steps)
+        ref_state = r.state(h, sc.n)
+    finally:
+        r.destroy(h)
+    ref = sc.n * steps / ref_s
+    return {"scene": "1,048,576-sphere box scene as above with spring 0.25 (stable under the reference scheme)",
+            "steps": f"{warm + 1}..{warm + steps}", "reference_ms_per_step": 1e3 * ref_s / steps,
+            "reference_particle_steps_per_s": ref, "reference_dtype": "f64",
+            "reference_finite_at_end": bool(np.isfinite(ref_state).all()),
+            "ours": ours,
+            "speedup_f32": ours["f32"]["particle_steps_per_s"] / ref,
+            "speedup_f64": ours["f64"]["particle_steps_per_s"] / ref}
+
+
 # Secondary measurements.  The reference's contact kick k*overlap/m is not
 # scaled by dt, so the scheme is stable only for k*dt/m below about 1.  The
 # differentiation and batch scenes with their specified springs (k*dt/m = 373
@@ -428,17 +479,29 @@ def run_ours(args, world, rank, local, dist):
     cells = int(g.n_cells)
     block = max(1, args.block)
 
+    def blocks_of(total: int) -> list[int]:
+        return [min(block, total - k) for k in range(0, total, block)]
+
     def timed_steps(total: int) -> tuple[float, int]:
-        ms, launches, left = 0.0, 0, total
-        while left > 0:
-            b = min(block, left)
+        ms, launches = 0.0, 0
+        for b in blocks_of(total):
             sim.checkpoint_load(0)
             ms += sim.time_steps(b)
             launches += sim.launches()
-            left -= b
         return ms, launches
 
-    timed_steps(max(args.warmup, 3))
+    # Warm-up: every block length the timed region uses runs once first, so
+    # each CUDA graph is captured and instantiated outside the timed region;
+    # then whole blocks until at least max(warmup, 3) steps have run.
+    warm_lens = sorted(set(blocks_of(args.steps)))
+    warmed = 0
+    for b in warm_lens:
+        timed_steps(b)
+        warmed += b
+    while warmed < max(args.warmup, 3):
+        b = warm_lens[-1]
+        timed_steps(b)
+        warmed += b
     barrier(dist)
     sim.sync()
     with ClockSampler(local) as clk:
@@ -462,9 +525,10 @@ def run_ours(args, world, rank, local, dist):
     step_ms = dev_ms / args.steps
     step_gbs = step_alg_bytes(n, cells) / (step_ms * 1e-3) / 1e9
 
-    # end to end through host buffers: upload, block steps, download
-    e2e_iters = max(1, min(args.steps // block, 5))
-    # host buffers in pinned memory, as an application streaming states would hold them
+    # End to end through the C ABI with host buffers: for every block of the
+    # same decomposition as `value`, upload the scene's initial state from
+    # pinned host memory, run the block, download the state.  One untimed
+    # pass first (pinned-memory paths, graphs already captured above).
     import torch
 
     pin_in = torch.empty((n, 8), dtype=torch.float64, pin_memory=True)
@@ -472,28 +536,29 @@ def run_ours(args, world, rank, local, dist):
     host = pin_in.numpy()
     host[:] = sc.state
     host_out = pin_out.numpy()
-    t_e2e = 0.0
-    for _ in range(e2e_iters + 1):
-        t0 = time.perf_counter()
-        sim.set_state(host)
-        sim.step(block)
-        out = sim.get_state(out=host_out)
-        dt = time.perf_counter() - t0
-        if _ > 0:  # first iteration warms the upload path
-            t_e2e += dt
-    e2e_value = sum_over_ranks(dist, float(n * block * e2e_iters)) / max_over_ranks(dist, t_e2e)
-    del out
 
-    state_bytes = n * (4 * 2 * 16 + 4 * 4) + 2 * 4 * (cells + 1)
+    def e2e_pass() -> float:
+        sim.sync()
+        t0 = time.perf_counter()
+        for b in blocks_of(args.steps):
+            sim.set_state(host)
+            sim.step(b)
+            sim.get_state(out=host_out)
+        return time.perf_counter() - t0
+
+    e2e_pass()
+    barrier(dist)
+    t_e2e = e2e_pass()
+    e2e_value = sum_over_ranks(dist, float(n * args.steps)) / max_over_ranks(dist, t_e2e)
+    n_blocks = len(blocks_of(args.steps))
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "f32" else "f64",
         "data": "synthetic: seeded generator of the 1M-sphere scene (numpy default_rng(2))",
-        "config": {"workload": WORKLOAD, "n_particles": n, "grid": [g.nb[0], g.nb[1], g.nb[2]], "cells": cells,
-                   "block": block, "state_restored_every": block,
-                   "l2": f"working set {state_bytes / 2**20:.0f} MiB > 126 MiB L2; no flush",
-                   "parallelism": f"{world} independent replicas (one per GPU, no collective)"},
+        "config": bench_config(n, block, world),
+        "grid": {"cells_per_axis": [g.nb[0], g.nb[1], g.nb[2]], "cells": cells, "cell_edge": "2 r_max"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": CONTACTS_TRAFFIC if (dom == "contacts" and args.precision == "f32") else None,
@@ -503,10 +568,10 @@ def run_ours(args, world, rank, local, dist):
         "step_roofline": {"alg_bytes_per_step": step_alg_bytes(n, cells), "achieved_gbs": step_gbs,
                           "frac": step_gbs / peak},
         "kernels_ms_per_step": {k: v[0] for k, v in per_step.items()},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 64.0 * n / block,
-                "d2h_bytes_per_step": 64.0 * n / block,
-                "how": f"ps_set_state(pinned host) + ps_step({block}) + ps_get_state(pinned host), wall clock, "
-                       f"{e2e_iters} blocks"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 64.0 * n * n_blocks / args.steps,
+                "d2h_bytes_per_step": 64.0 * n * n_blocks / args.steps,
+                "how": f"per block of the same {args.steps} steps: ps_set_state(pinned host, 64 B per sphere) + "
+                       f"ps_step(block) + ps_get_state(pinned host), wall clock, max over ranks"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "wall_s": wall,
@@ -517,25 +582,79 @@ def run_ours(args, world, rank, local, dist):
             line[name] = EXTRAS[name](psb200, scenes, local, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = reference_cpu_sample(sc, args.cpu_budget, 20)
+    if rank == 0 and world == 1 and not args.no_reference_cuda:
+        line["reference_cuda"] = reference_cuda_measure(psb200, scenes, local)
     return line
 
 
+def bench_config(n: int, block: int, world: int) -> dict:
+    """The workload description shared by both arms."""
+    return {"workload": WORKLOAD, "n_particles": n, "block": block, "state_restored_every": block,
+            "timed_steps": "steps 1..block of the scene in every block (initial state restored between blocks)",
+            "l2": "working set 205 MiB (FP32 state, cell arrays) > 126 MiB L2; no flush",
+            "parallelism": f"{world} independent replicas (one per GPU, no collective)"}
+
+
 def run_reference(args, world, rank):
-    """Reference arm: the reference's own CPU simulator on the same scene."""
+    """Reference arm: the reference's own CPU simulator (oracle/_ref/
+    libref_cpu.so, built from its unmodified sources) on the same scene and
+    the same block decomposition as this library's arm: every block starts
+    from the scene's initial state (a fresh simulator; construction
+    untimed).  The reference's box-container path is serial, so one host
+    thread is all it can use.  Warm-up: `--warmup` whole steps on a
+    simulator of their own (at most about a minute of them); timed: the
+    `--steps` steps, or as many whole steps as fit `--ref-budget` seconds."""
+    from oracle import ps_oracle as O
     from psb200 import scenes
 
     if rank != 0:
         return None
     sc = scenes.c2_scene()
-    s = reference_cpu_sample(sc, args.cpu_budget, max(1, args.steps), warmup=min(args.warmup, 1))
-    return {"impl": "reference", "metric": METRIC, "value": s["value"], "unit": UNIT, "n_gpus": world,
-            "steps": s["steps"], "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * s["seconds"] / s["steps"],
+    block = max(1, args.block)
+    blocks = [min(block, args.steps - k) for k in range(0, args.steps, block)]
+    if os.path.exists(O.REF_CPU_SO):
+        r, kind = O.ref_cpu(), "reference"
+    else:
+        r, kind = None, "port"
+    warm_done, warm_t = 0, 0.0
+    steps_done, t = 0, 0.0
+    if r is not None:
+        h = r.create(sc)
+        while warm_done < args.warmup and warm_t < 60.0:
+            warm_t += r.time_steps(h, 1)
+            warm_done += 1
+        r.destroy(h)
+        for b in blocks:
+            if t >= args.ref_budget:
+                break
+            h = r.create(sc)
+            k = 0
+            while k < b and t < args.ref_budget:
+                t += r.time_steps(h, 1)
+                k += 1
+            steps_done += k
+            r.destroy(h)
+    else:
+        # the oracle (C restatement of the same scheme), one thread
+        t0 = time.perf_counter()
+        while steps_done < args.steps and time.perf_counter() - t0 < args.ref_budget:
+            O.run(sc, 1, "f64")
+            steps_done += 1
+        t = time.perf_counter() - t0
+    value = sc.n * steps_done / t
+    sample = (f"{steps_done} whole steps of the 1M-sphere scene in blocks of {block} from its initial state "
+              f"({t:.1f} s timed, one thread: the reference's box path is serial)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": steps_done, "warmup": warm_done, "ms_per_step": 1e3 * t / steps_done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded generator of the 1M-sphere scene (numpy default_rng(2))",
-            "config": {"workload": WORKLOAD, "n_particles": sc.n,
-                       "note": f"{s['steps']} of the requested {args.steps} steps fit the time budget"},
-            "cpu_baseline": {k: s[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": s["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": bench_config(sc.n, block, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if steps_done < args.steps or warm_done < args.warmup:
+        line["note"] = (f"{steps_done} of the requested {args.steps} steps and {warm_done} of {args.warmup} warm-up "
+                        f"steps fit the time budget")
+    return line
 
 
 def main():
@@ -548,6 +667,10 @@ def main():
     ap.add_argument("--block", type=int, default=100, help="steps per block; the state is restored between blocks")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of reference CPU stepping")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip the head-to-head with the reference's own CUDA build")
+    ap.add_argument("--ref-budget", type=float, default=240.0,
+                    help="seconds of timed reference CPU stepping in the --impl reference arm")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint, batch and mesh measurements")
     ap.add_argument("--extra", choices=sorted(EXTRAS),
