@@ -115,6 +115,8 @@ struct ps_sim {
 
   std::map<int64_t, cudaGraphExec_t> graphs;
   int64_t graph_block = 200;  // steps per captured CUDA graph (ps_autotune may change it)
+  int32_t walk = WALK_WARP;   // neighbour walk of the contact kernel (WALK_LANE / WALK_WARP)
+  int32_t contact_block = 256;  // threads per CTA of the contact kernel (WALK_WARP: 128, 256, 512; WALK_LANE: 256)
   int64_t last_launches = 0;
   std::map<int32_t, void*> checkpoints;  // slot -> device copy of (P0, V1, orig)
   cudaAccessPolicyWindow l2_window{};     // count + offset arrays kept in L2
@@ -214,6 +216,39 @@ unsigned move_blocks(int64_t n, uint32_t words) {
   return (unsigned)std::max<int64_t>((n + per - 1) / per, (words + STEP_THREADS - 1) / STEP_THREADS);
 }
 
+static_assert(WALK_LANE == PS_WALK_LANE && WALK_WARP == PS_WALK_WARP, "walk ids of the C ABI");
+
+// Contact kernel variants the tuner times: {walk, threads per CTA}, in the
+// order of ps_tune_result::contact_ms.
+constexpr int kContactConfigs = 4;
+constexpr int32_t kContactConfig[kContactConfigs][2] = {
+    {WALK_LANE, 256}, {WALK_WARP, 128}, {WALK_WARP, 256}, {WALK_WARP, 512}};
+
+// The contact kernel of the simulation's neighbour walk and CTA size
+// (ps_set_contact_kernel, ps_autotune).
+template <class T, bool MULTI, bool MESH, bool FUSED>
+struct ContactLaunch {
+  void (*fn)(StepBufs<T>, SceneParams<T>, const MeshView*);
+  unsigned block;
+  unsigned grid;
+};
+
+template <class T, bool MULTI, bool MESH, bool FUSED>
+ContactLaunch<T, MULTI, MESH, FUSED> contacts_kernel(const ps_sim* s) {
+  ContactLaunch<T, MULTI, MESH, FUSED> c;
+  if (s->walk == WALK_LANE) {
+    c = {k_contacts<T, MULTI, MESH, FUSED, WALK_LANE, 256>, 256u, 0u};
+  } else if (s->contact_block == 128) {
+    c = {k_contacts<T, MULTI, MESH, FUSED, WALK_WARP, 128>, 128u, 0u};
+  } else if (s->contact_block == 512) {
+    c = {k_contacts<T, MULTI, MESH, FUSED, WALK_WARP, 512>, 512u, 0u};
+  } else {
+    c = {k_contacts<T, MULTI, MESH, FUSED, WALK_WARP, 256>, 256u, 0u};
+  }
+  c.grid = (unsigned)((s->n_total + c.block - 1) / c.block);
+  return c;
+}
+
 // ---- the launch sequence -----------------------------------------------------
 template <class T, bool MULTI, bool MESH>
 int64_t enqueue_steps(ps_sim* s, int64_t steps) {
@@ -235,10 +270,13 @@ int64_t enqueue_steps(ps_sim* s, int64_t steps) {
     pdl_launch(k_scatter, move_blocks(s->n_total, b.n_tiles), STEP_THREADS, st, (const uint32_t*)s->cell, s->slot,
                (const uint32_t*)s->orig, (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles);
     pdl_launch(k_rank_move<T>, move_blocks(s->n_total, 0), STEP_THREADS, st, b);
-    if (k + 1 < steps)
-      pdl_launch(k_contacts<T, MULTI, MESH, true>, gp, STEP_THREADS, st, b, sp0, mv);
-    else
-      pdl_launch(k_contacts<T, MULTI, MESH, false>, gp, STEP_THREADS, st, b, sp0, mv);
+    if (k + 1 < steps) {
+      const auto c = contacts_kernel<T, MULTI, MESH, true>(s);
+      pdl_launch(c.fn, c.grid, c.block, st, b, sp0, mv);
+    } else {
+      const auto c = contacts_kernel<T, MULTI, MESH, false>(s);
+      pdl_launch(c.fn, c.grid, c.block, st, b, sp0, mv);
+    }
     launches += 4;
   }
   return launches;
@@ -279,10 +317,13 @@ void enqueue_steps_recorded(ps_sim* s, int64_t steps, std::vector<LaunchRecord>&
     k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
     post();
     pre(PS_K_CONTACTS);
-    if (k + 1 < steps)
-      k_contacts<T, MULTI, MESH, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
-    else
-      k_contacts<T, MULTI, MESH, false><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+    if (k + 1 < steps) {
+      const auto c = contacts_kernel<T, MULTI, MESH, true>(s);
+      c.fn<<<c.grid, c.block, 0, st>>>(b, sp0, s->d_mesh_view);
+    } else {
+      const auto c = contacts_kernel<T, MULTI, MESH, false>(s);
+      c.fn<<<c.grid, c.block, 0, st>>>(b, sp0, s->d_mesh_view);
+    }
     post();
   }
 }
@@ -1054,10 +1095,13 @@ int enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes, 
     b.tape_vpre = row.vpre;
     b.tape_cell = row.cell;
     const MeshView* mv = s->d_mesh_view;
-    if (k + 1 < steps)
-      pdl_launch(k_contacts<T, MULTI, false, true>, gp, STEP_THREADS, st, b, sp0, mv);
-    else
-      pdl_launch(k_contacts<T, MULTI, false, false>, gp, STEP_THREADS, st, b, sp0, mv);
+    if (k + 1 < steps) {
+      const auto c = contacts_kernel<T, MULTI, false, true>(s);
+      pdl_launch(c.fn, c.grid, c.block, st, b, sp0, mv);
+    } else {
+      const auto c = contacts_kernel<T, MULTI, false, false>(s);
+      pdl_launch(c.fn, c.grid, c.block, st, b, sp0, mv);
+    }
   }
   return PS_OK;
 }
@@ -1629,6 +1673,28 @@ extern "C" int ps_autotune(ps_sim* s, int64_t trial_steps, const double* cell_fa
   for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
   s->graphs.clear();
   s->graph_block = best_l;
+  // then the contact kernel on the chosen grid and graph length: the walk
+  // and its CTA size (the summation order depends on neither)
+  int32_t best_walk = s->walk, best_cb = s->contact_block;
+  double best_k = INFINITY;
+  for (int32_t v = 0; v < kContactConfigs && rc == PS_OK; ++v) {
+    s->walk = kContactConfig[v][0];
+    s->contact_block = kContactConfig[v][1];
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    double ms = 0.0;
+    rc = trial(ms);
+    out->contact_ms[v] = ms;
+    if (rc == PS_OK && ms < best_k) {
+      best_k = ms;
+      best_walk = s->walk;
+      best_cb = s->contact_block;
+    }
+  }
+  s->walk = best_walk;
+  s->contact_block = best_cb;
+  for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
   if (rc == PS_OK) rc = load_state(s, saved);
   if (rc == PS_OK) rc = ps_sync(s);
   cudaEventDestroy(ea);
@@ -1637,8 +1703,33 @@ extern "C" int ps_autotune(ps_sim* s, int64_t trial_steps, const double* cell_fa
   if (rc != PS_OK) return rc;
   out->cell_factor = best_f;
   out->graph_block = best_l;
-  out->ms_per_step = best;
+  out->ms_per_step = std::min(best, best_k);
   out->before_ms_per_step = before;
+  out->contact_walk = best_walk;
+  out->contact_block = best_cb;
+  return PS_OK;
+}
+
+extern "C" int ps_set_contact_kernel(ps_sim* s, int32_t walk, int32_t block) {
+  if (s == nullptr) return fail(PS_ERR_INVALID, "ps_set_contact_kernel: null simulation");
+  bool ok = false;
+  for (int32_t v = 0; v < kContactConfigs; ++v) ok = ok || (kContactConfig[v][0] == walk && kContactConfig[v][1] == block);
+  if (!ok)
+    return fail(PS_ERR_INVALID, "ps_set_contact_kernel: walk/block must be PS_WALK_LANE/256 or PS_WALK_WARP/128, 256, 512");
+  if (walk != s->walk || block != s->contact_block) {
+    DeviceGuard guard(s->device);
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);  // they hold the previous kernel
+    s->graphs.clear();
+    s->walk = walk;
+    s->contact_block = block;
+  }
+  return PS_OK;
+}
+
+extern "C" int ps_get_contact_kernel(ps_sim* s, int32_t* walk, int32_t* block) {
+  if (s == nullptr || walk == nullptr || block == nullptr) return fail(PS_ERR_INVALID, "ps_get_contact_kernel: bad argument");
+  *walk = s->walk;
+  *block = s->contact_block;
   return PS_OK;
 }
 

@@ -364,46 +364,177 @@ __device__ __forceinline__ void cell_coords(uint32_t c, const SceneParams<T>& sp
   cy = (int32_t)(col - (uint32_t)cx * (uint32_t)sp.nb[1]);
 }
 
-template <class T, bool MULTI, bool MESH, bool FUSED>
-__global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 4 : 3) k_contacts(StepBufs<T> b, SceneParams<T> sp0,
-                                                                                  const MeshView* mv) {
-  const uint32_t i = blockIdx.x * STEP_THREADS + threadIdx.x;
+// Register shuffle of a whole state vector from lane `src`.
+template <class T>
+__device__ __forceinline__ vec4_t<T> shfl4(const vec4_t<T>& v, int src) {
+  vec4_t<T> r;
+  r.x = __shfl_sync(0xffffffffu, v.x, src);
+  r.y = __shfl_sync(0xffffffffu, v.y, src);
+  r.z = __shfl_sync(0xffffffffu, v.z, src);
+  r.w = __shfl_sync(0xffffffffu, v.w, src);
+  return r;
+}
+
+// Walk of the neighbour columns by the whole warp (WALK_WARP).
+//
+// Every lane's range [mylo, myhi) in a neighbour column lies inside the
+// warp's union [ulo, uhi) of that column: the 32 lanes hold consecutive
+// sorted slots, so their ranges in the same neighbour column overlap or
+// abut, and the union is about a warp's worth of candidates (28.8 on
+// average, at most 67, on the 1M-sphere scene).  The union is read in
+// windows of 32 * walk_window() slots, walk_window() coalesced loads per
+// lane, lane l holding slots base + l + 32 k; each lane takes its own
+// candidates from the holders by register shuffle, in ascending slot order.
+// That is the per-lane order of the nine-loop walk, so every sum is
+// bit-identical to it.
+//
+// Loads per lane and window, and columns whose first window is in flight
+// while the current column is walked.  FP64 holds half as many: a double4
+// window per lane is 8 registers.
+template <class T>
+__host__ __device__ constexpr int walk_window() {
+  return sizeof(T) == 4 ? 2 : 1;
+}
+template <class T>
+__host__ __device__ constexpr int walk_ahead() {
+  return sizeof(T) == 4 ? 2 : 1;
+}
+
+template <class T>
+struct Window {
+  vec4_t<T> c[walk_window<T>()];
+};
+
+// Slots [base, base + 32 walk_window()) of a union ending at `end` (zeros
+// past it; an empty union has base >= end).
+template <class T>
+__device__ __forceinline__ Window<T> load_window(const vec4_t<T>* __restrict__ P0, uint32_t base, uint32_t end,
+                                                 unsigned lane) {
+  Window<T> w;
+#pragma unroll
+  for (int k = 0; k < walk_window<T>(); ++k) {
+    const uint32_t j = base + lane + 32u * k;
+    if (base < end && j < end) {
+      w.c[k] = ld4<T>(P0 + j);
+    } else {
+      w.c[k].x = w.c[k].y = w.c[k].z = w.c[k].w = T(0);
+    }
+  }
+  return w;
+}
+
+template <class T>
+__device__ __forceinline__ void walk_column(const vec4_t<T>* __restrict__ P0, const vec4_t<T>* __restrict__ V0,
+                                            uint32_t i, unsigned lane, uint32_t mylo, uint32_t myhi, uint32_t ulo,
+                                            uint32_t uhi, Window<T> win, const vec4_t<T>& P, const vec4_t<T>& Vi,
+                                            T ks, T es, T& vx, T& vy, T& vz) {
+  for (uint32_t wbase = ulo; wbase < uhi; wbase += 32u * walk_window<T>()) {  // warp-uniform
+    if (wbase != ulo) win = load_window<T>(P0, wbase, uhi, lane);
+#pragma unroll
+    for (int k = 0; k < walk_window<T>(); ++k) {
+      const uint32_t base = wbase + 32u * k;
+      const uint32_t a = mylo > base ? mylo : base;
+      const uint32_t e = myhi < base + 32u ? myhi : base + 32u;
+      const uint32_t cnt = e > a ? e - a : 0u;
+      const uint32_t mx = __reduce_max_sync(0xffffffffu, cnt);
+      for (uint32_t t = 0; t < mx; ++t) {
+        // for t < cnt the holder of slot a + t is lane a - base + t < 32
+        const vec4_t<T> Pj = shfl4<T>(win.c[k], (int)((a - base + t) & 31u));
+        const uint32_t j = a + t;
+        if (t < cnt && j != i) contact_one<T>(V0, j, P, Vi, Pj, ks, es, vx, vy, vz);
+      }
+    }
+  }
+}
+
+// Neighbour walk of k_contacts.
+//   WALK_LANE: each thread loops over its own nine slot ranges.
+//   WALK_WARP: the warp walks each column's union range together
+//              (walk_column), with the first windows of the next
+//              walk_ahead() columns loaded ahead, so a warp waits for a few
+//              rounds of coalesced loads instead of one per candidate.
+// Both apply the same candidates in the same order.
+enum : int { WALK_LANE = 0, WALK_WARP = 1 };
+
+// Resident CTAs per SM the contact kernel is compiled for: 1,024 threads
+// per SM in FP32 (64 registers) and 768 in FP64 (85 registers), whatever
+// the CTA size.
+template <class T, int BLOCK>
+__host__ __device__ constexpr int contact_min_blocks() {
+  return (sizeof(T) == 4 ? 1024 : 768) / BLOCK > 0 ? (sizeof(T) == 4 ? 1024 : 768) / BLOCK : 1;
+}
+
+template <class T, bool MULTI, bool MESH, bool FUSED, int WALK, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, contact_min_blocks<T, BLOCK>()) k_contacts(StepBufs<T> b, SceneParams<T> sp0,
+                                                                                    const MeshView* mv) {
+  const uint32_t i = blockIdx.x * BLOCK + threadIdx.x;
   const bool valid = i < b.n;
   uint32_t c = 0;
   pdl_wait();
+  // Lanes past the end walk empty ranges: the warp's shuffles and the
+  // count's ballot need every lane.
+  const SceneParams<T>& sp = scene_of<T, MULTI>(valid ? i : 0u, sp0, b.scenes, b.pbase, b.n_scenes);
+  vec4_t<T> P, Vi;
+  uint32_t my_cell = sp.cbase;
   if (valid) {
-    const SceneParams<T>& sp = scene_of<T, MULTI>(i, sp0, b.scenes, b.pbase, b.n_scenes);
-    vec4_t<T> P = b.P0[i];
-    const vec4_t<T> Vi = b.V0[i];
-    T vx = Vi.x, vy = Vi.y, vz = Vi.z;
-    int32_t cx, cy, cz;
-    cell_coords<T>(b.scell[i], sp, cx, cy, cz);
-    const int32_t nx = sp.nb[0], ny = sp.nb[1], nz = sp.nb[2];
-    const uint32_t z0 = (uint32_t)(cz > 0 ? cz - 1 : 0);
-    const uint32_t z1 = (uint32_t)(cz + 1 < nz ? cz + 1 : nz - 1) + 1u;
-    // A particle whose own position is not finite has no contact: every
-    // pair gives d2 = inf (rejected by the filter) or NaN (overlap NaN), so
-    // its candidate loop is skipped.  Diverged particles all hash to a few
-    // cells, where the loop would otherwise be quadratic.
-    const bool live = isfinite(P.x) && isfinite(P.y) && isfinite(P.z);
-    uint32_t lo[9], hi[9];
+    P = b.P0[i];
+    Vi = b.V0[i];
+    my_cell = b.scell[i];
+  } else {
+    P.x = P.y = P.z = P.w = T(0);
+    Vi = P;
+  }
+  T vx = Vi.x, vy = Vi.y, vz = Vi.z;
+  int32_t cx, cy, cz;
+  cell_coords<T>(my_cell, sp, cx, cy, cz);
+  const int32_t nx = sp.nb[0], ny = sp.nb[1], nz = sp.nb[2];
+  const uint32_t z0 = (uint32_t)(cz > 0 ? cz - 1 : 0);
+  const uint32_t z1 = (uint32_t)(cz + 1 < nz ? cz + 1 : nz - 1) + 1u;
+  // A particle whose own position is not finite has no contact: every
+  // pair gives d2 = inf (rejected by the filter) or NaN (overlap NaN), so
+  // its candidate loop is skipped.  Diverged particles all hash to a few
+  // cells, where the loop would otherwise be quadratic.
+  const bool live = valid && isfinite(P.x) && isfinite(P.y) && isfinite(P.z);
+  uint32_t lo[9], hi[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      const int32_t bx = cx - 1 + q / 3, by = cy - 1 + q % 3;
-      const bool ok = live && bx >= 0 && bx < nx && by >= 0 && by < ny;
-      // in-range address even where the column does not exist
-      const uint32_t col = ok ? sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz : sp.cbase;
-      lo[q] = ok ? __ldg(b.offset + col + z0) : 0u;
-      hi[q] = ok ? __ldg(b.offset + col + z1) : 0u;
-    }
+  for (int q = 0; q < 9; ++q) {
+    const int32_t bx = cx - 1 + q / 3, by = cy - 1 + q % 3;
+    const bool ok = live && bx >= 0 && bx < nx && by >= 0 && by < ny;
+    // in-range address even where the column does not exist
+    const uint32_t col = ok ? sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz : sp.cbase;
+    lo[q] = ok ? __ldg(b.offset + col + z0) : 0u;
+    hi[q] = ok ? __ldg(b.offset + col + z1) : 0u;
+  }
+  const T ks = sp.k_spring, es = sp.e_sphere;
+  if constexpr (WALK == WALK_LANE) {
     // visit the nine ranges in canonical order
-    const T ks = sp.k_spring, es = sp.e_sphere;
 #pragma unroll
     for (int q = 0; q < 9; ++q)
       for (uint32_t j = lo[q]; j < hi[q]; ++j) {
         if (j == i) continue;
         contact_one<T>(b.V0, j, P, Vi, ld4<T>(b.P0 + j), ks, es, vx, vy, vz);
       }
+  } else {
+    const unsigned lane = threadIdx.x & 31u;
+    // union bounds of each column, taken when its first window is loaded
+    uint32_t ulo[9], uhi[9];
+    Window<T> win[9];
+    constexpr int AHEAD = walk_ahead<T>();
+#pragma unroll
+    for (int q = 0; q < 9 + AHEAD; ++q) {
+      if (q < 9) {
+        const bool has = lo[q] < hi[q];
+        ulo[q] = __reduce_min_sync(0xffffffffu, has ? lo[q] : 0xffffffffu);
+        uhi[q] = __reduce_max_sync(0xffffffffu, has ? hi[q] : 0u);
+        win[q] = load_window<T>(b.P0, ulo[q], uhi[q], lane);
+      }
+      if (q >= AHEAD) {
+        const int w = q - AHEAD;
+        walk_column<T>(b.P0, b.V0, i, lane, lo[w], hi[w], ulo[w], uhi[w], win[w], P, Vi, ks, es, vx, vy, vz);
+      }
+    }
+  }
+  if (valid) {
     vec4_t<T> V = Vi;
     V.x = vx;
     V.y = vy;

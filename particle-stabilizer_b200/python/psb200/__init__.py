@@ -27,7 +27,7 @@ EXPORTED = (
     "ps_grid_get", "ps_buckets_get", "ps_last_launch_count", "ps_destroy", "ps_simulate",
     "ps_exclusive_scan_scratch_bytes", "ps_exclusive_scan_u32", "ps_read_csv", "ps_write_csv", "ps_read_obj",
     "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "ps_forward_checkpointed",
-    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_autotune", "ps_set_neighbor_lists", "ps_list_stats", "ps_tune_neighbor_lists",
+    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_autotune", "ps_set_contact_kernel", "ps_get_contact_kernel", "ps_set_neighbor_lists", "ps_list_stats", "ps_tune_neighbor_lists",
     "ps_resolve_overlaps", "ps_overlap_stats",
     "ps_write_obj_spheres", "runSimulateCUDA",
 )
@@ -62,7 +62,13 @@ class Grad(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("cell_factor", C.c_double), ("graph_block", C.c_int64), ("ms_per_step", C.c_double),
-                ("before_ms_per_step", C.c_double)]
+                ("before_ms_per_step", C.c_double), ("contact_walk", C.c_int32), ("contact_block", C.c_int32),
+                ("contact_ms", C.c_double * 4)]
+
+
+WALK_LANE, WALK_WARP = 0, 1
+# contact kernel variants in the order of TuneResult.contact_ms: (walk, threads per CTA)
+CONTACT_KERNELS = ((WALK_LANE, 256), (WALK_WARP, 128), (WALK_WARP, 256), (WALK_WARP, 512))
 
 
 class PSError(RuntimeError):
@@ -113,6 +119,8 @@ def lib() -> C.CDLL:
                                           C.POINTER(C.c_double)]
         L.ps_overlap_stats.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
         L.ps_write_obj_spheres.argtypes = [C.c_char_p, C.c_void_p, C.c_int64]
+        L.ps_set_contact_kernel.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+        L.ps_get_contact_kernel.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.ps_autotune.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
                                   C.POINTER(TuneResult)]
         _lib = L
@@ -281,7 +289,18 @@ class Simulation:
         return {"cell_factor": res.cell_factor, "graph_block": int(res.graph_block),
                 "ms_per_step": res.ms_per_step, "before_ms_per_step": res.before_ms_per_step,
                 "cell_factors": [float(x) for x in f], "graph_blocks": [int(x) for x in b],
-                "ms_table": table.tolist()}
+                "ms_table": table.tolist(), "contact_kernel": (int(res.contact_walk), int(res.contact_block)),
+                "contact_ms": [float(x) for x in res.contact_ms], "contact_kernels": list(CONTACT_KERNELS)}
+
+    def set_contact_kernel(self, walk: int, block: int) -> None:
+        """ps_set_contact_kernel: WALK_LANE with 256 threads per CTA, or
+        WALK_WARP with 128, 256 or 512 (identical results)."""
+        _check(lib().ps_set_contact_kernel(self.h, int(walk), int(block)), "ps_set_contact_kernel")
+
+    def contact_kernel(self) -> tuple[int, int]:
+        w, b = C.c_int32(), C.c_int32()
+        _check(lib().ps_get_contact_kernel(self.h, C.byref(w), C.byref(b)), "ps_get_contact_kernel")
+        return int(w.value), int(b.value)
 
     def backward(self, dl_dstate: np.ndarray):
         """Gradients of a loss of the final state: dl_dstate is (n, 6) =

@@ -1,7 +1,9 @@
-"""ps_autotune: the cell-size factor and graph block chosen by timing, on a
-batch of three scenes.  The tuner must restore the state it started from,
-report a full timing table, and leave a simulation whose trajectories are
-exactly the oracle's with the chosen cell sizes (bit for bit, FP32)."""
+"""ps_autotune: the cell-size factor, graph block and contact kernel (walk
+and CTA size) chosen by timing, on a batch of three scenes.  The tuner must
+restore the state it started from, report full timing tables, and leave a
+simulation whose trajectories are exactly the oracle's with the chosen cell
+sizes (bit for bit, FP32).  Every contact kernel variant gives the same
+states bit for bit."""
 import numpy as np
 import pytest
 
@@ -22,7 +24,10 @@ def test_autotune_choice_restores_state_and_keeps_parity(need_gpu):
         table = np.array(res["ms_table"])
         assert table.shape == (3, 2) and np.all(table > 0) and res["before_ms_per_step"] > 0
         assert res["cell_factor"] in factors and res["graph_block"] in blocks
-        assert res["ms_per_step"] == table.min()
+        assert res["ms_per_step"] == min(table.min(), min(res["contact_ms"]))
+        assert len(res["contact_ms"]) == 4 and min(res["contact_ms"]) > 0
+        assert res["contact_kernel"] == psb200.CONTACT_KERNELS[int(np.argmin(res["contact_ms"]))]
+        assert sim.contact_kernel() == res["contact_kernel"]
         assert np.array_equal(sim.get_state(), before)
         grids = [sim.grid(k) for k in range(len(batch))]
         sim.step(30)
@@ -36,6 +41,31 @@ def test_autotune_choice_restores_state_and_keeps_parity(need_gpu):
         off += sc.n
 
 
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_every_contact_kernel_gives_the_same_states(need_gpu, precision):
+    """The four contact kernels (per-lane walk with 256 threads per CTA,
+    warp walk with 128, 256 and 512) on a batch of a dense pile, a sparse
+    lattice and a triangle container: states bit-identical to each other
+    and to the oracle after 40 steps."""
+    batch = [scenes.pile(1500, seed=41, k_spring=1.0), scenes.lattice_c1(side=10), scenes.box_mesh_scene()]
+    states = []
+    for walk, block in psb200.CONTACT_KERNELS:
+        with psb200.Simulation(batch, precision) as sim:
+            sim.set_contact_kernel(walk, block)
+            assert sim.contact_kernel() == (walk, block)
+            sim.set_state()
+            sim.step(40)
+            states.append(sim.get_state())
+    for st in states[1:]:
+        assert np.array_equal(st, states[0])
+    off = 0
+    for sc in batch:
+        want = O.run(sc, 40, precision)
+        got = states[0][off:off + sc.n]
+        assert np.array_equal(got.astype(np.float32) if precision == "f32" else got, want)
+        off += sc.n
+
+
 def test_autotune_rejects_bad_arguments(need_gpu):
     sc = scenes.pile(100, seed=3)
     with psb200.Simulation(sc, "f32") as sim:
@@ -46,3 +76,7 @@ def test_autotune_rejects_bad_arguments(need_gpu):
             sim.autotune(trial_steps=2, cell_factors=(0.5,))
         with pytest.raises(psb200.PSError, match="bad argument"):
             sim.autotune(trial_steps=0)
+        with pytest.raises(psb200.PSError, match="walk/block"):
+            sim.set_contact_kernel(psb200.WALK_LANE, 128)
+        with pytest.raises(psb200.PSError, match="walk/block"):
+            sim.set_contact_kernel(psb200.WALK_WARP, 1024)
