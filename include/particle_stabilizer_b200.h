@@ -281,13 +281,24 @@ int ps_exclusive_scan_u32(const uint32_t* d_in, uint32_t* d_out, int64_t n, void
  * fixed array inside this library (128 KB per GPU, held from the moment the
  * library is loaded on that GPU until the process exits), so n is limited to
  * PS_SCAN_NOALLOC_MAX_N elements; larger n returns PS_ERR_INVALID.  The first
- * call on each device looks up the array's device address; make that first
+ * call in each CUDA context (the device's primary context, or a context of
+ * the caller's own) looks up the array's device address; make that first
  * call before any stream capture.  Every call on a device shares the one
  * array, so calls whose kernels may overlap on the GPU (different streams
  * without ordering) race and give wrong results: order them on one stream.
- * d_in may equal d_out. */
+ * d_in may equal d_out.  A look-back wait that gives up (a bounded wait; it
+ * never hangs) leaves a wrong prefix and records PS_DEVERR_SCAN_TIMEOUT in a
+ * device word that ps_exclusive_scan_u32_noalloc_status reports. */
 #define PS_SCAN_NOALLOC_MAX_N 134217728LL
 int ps_exclusive_scan_u32_noalloc(const uint32_t* d_in, uint32_t* d_out, int64_t n, void* stream);
+
+/* Device error bits recorded by ps_exclusive_scan_u32_noalloc calls in the
+ * current CUDA context since the previous status query: 0 when every scan
+ * was complete, PS_DEVERR_SCAN_TIMEOUT (1) when a look-back wait gave up
+ * and that call's prefix is wrong.  Waits for the work queued on `stream`,
+ * so query on the stream the scans ran on; clears the bits.  Allocates
+ * nothing.  No counterpart in the reference. */
+int ps_exclusive_scan_u32_noalloc_status(void* stream, uint32_t* device_error);
 
 /* CSV particle file, the reference's format (src/ParticleStabilizer/ParticleIO.cpp:58-144):
  * header line skipped; rows x,y,z,r; mass = density*4/3*pi*r^3; velocity is

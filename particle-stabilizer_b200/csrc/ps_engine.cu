@@ -16,6 +16,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1977,23 +1978,81 @@ extern "C" int ps_exclusive_scan_u32(const uint32_t* d_in, uint32_t* d_out, int6
 }
 
 // ---- exclusive scan that allocates nothing -------------------------------------
-// Scratch for ps_exclusive_scan_u32_noalloc: the ticket/error words and one
-// status word per tile, for at most PS_SCAN_NOALLOC_MAX_N elements.  Each GPU
+// Scratch for ps_exclusive_scan_u32_noalloc: the ticket word and one status
+// word per tile, for at most PS_SCAN_NOALLOC_MAX_N elements.  Each GPU
 // holds its own copy of this array from the moment the library is loaded on
 // it until the process exits.
 namespace {
 constexpr int64_t kNoAllocMaxTiles = PS_SCAN_NOALLOC_MAX_N / SCAN_TILE;  // 16384
-constexpr int kNoAllocMaxDevices = 64;
+constexpr int kNoAllocMaxContexts = 64;
 static_assert(PS_SCAN_NOALLOC_MAX_N % SCAN_TILE == 0, "whole tiles");
 }  // namespace
 
 static __device__ __align__(256) uint64_t g_noalloc_scan_scratch[1 + kNoAllocMaxTiles];
+// Device error bits (PS_DEVERR_SCAN_TIMEOUT) of every call since the last
+// ps_exclusive_scan_u32_noalloc_status on this GPU.  Kept apart from the
+// scratch array, which each call clears.
+static __device__ __align__(256) uint32_t g_noalloc_scan_error;
 
 namespace {
-// Device address of g_noalloc_scan_scratch per device, found on the first
-// call made with that device current (host code must not pass the symbol
-// itself: on the host it names a stand-in, not device memory).
-std::atomic<uint64_t*> g_noalloc_scratch_addr[kNoAllocMaxDevices];
+// Device addresses of the two arrays per CUDA context, found on the first
+// call made with that context current.  Host code must not pass the
+// symbols themselves: on the host they name stand-ins, not device memory.
+// Keyed by context rather than by device: a context of the caller's own, or
+// the primary context made again after cudaDeviceReset, holds its own copies.
+struct NoAllocAddrs {
+  void* ctx;
+  uint64_t* scratch;
+  uint32_t* err;
+};
+NoAllocAddrs g_noalloc_addrs[kNoAllocMaxContexts];
+int g_noalloc_n = 0;
+std::mutex g_noalloc_mu;
+
+using CtxGetCurrentFn = int (*)(void**);  // cuCtxGetCurrent, through the runtime's driver entry point
+
+void* current_context() {
+  static const CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  void* ctx = nullptr;
+  if (fn == nullptr || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+int noalloc_addrs(const char* who, uint64_t** scratch, uint32_t** err) {
+  void* ctx = current_context();
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (ctx != nullptr) {
+    for (int k = 0; k < g_noalloc_n; ++k)
+      if (g_noalloc_addrs[k].ctx == ctx) {
+        *scratch = g_noalloc_addrs[k].scratch;
+        *err = g_noalloc_addrs[k].err;
+        return PS_OK;
+      }
+  }
+  void *ps = nullptr, *pe = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&ps, g_noalloc_scan_scratch);
+  if (e == cudaSuccess) e = cudaGetSymbolAddress(&pe, g_noalloc_scan_error);
+  if (e != cudaSuccess || ps == nullptr || pe == nullptr)
+    return fail(PS_ERR_CUDA, std::string(who) + ": cudaGetSymbolAddress: " + cudaGetErrorString(e));
+  *scratch = static_cast<uint64_t*>(ps);
+  *err = static_cast<uint32_t*>(pe);
+  if (ctx == nullptr) ctx = current_context();  // the lookup made the device's primary context current
+  if (ctx != nullptr) {
+    if (g_noalloc_n == kNoAllocMaxContexts) {  // the oldest entry makes room
+      for (int m = 1; m < kNoAllocMaxContexts; ++m) g_noalloc_addrs[m - 1] = g_noalloc_addrs[m];
+      --g_noalloc_n;
+    }
+    g_noalloc_addrs[g_noalloc_n++] = {ctx, *scratch, *err};
+  }
+  return PS_OK;
+}
 }  // namespace
 
 extern "C" int ps_exclusive_scan_u32_noalloc(const uint32_t* d_in, uint32_t* d_out, int64_t n, void* stream) {
@@ -2004,25 +2063,30 @@ extern "C" int ps_exclusive_scan_u32_noalloc(const uint32_t* d_in, uint32_t* d_o
                                     " exceeds the fixed scratch capacity of " +
                                     std::to_string(PS_SCAN_NOALLOC_MAX_N) + " elements");
   if (n == 0) return PS_OK;
-  int dev = 0;
-  PS_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kNoAllocMaxDevices)
-    return fail(PS_ERR_INVALID, "ps_exclusive_scan_u32_noalloc: device id " + std::to_string(dev) + " out of range");
-  uint64_t* scratch = g_noalloc_scratch_addr[dev].load(std::memory_order_acquire);
-  if (scratch == nullptr) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scan_scratch);
-    if (e != cudaSuccess || p == nullptr)
-      return fail(PS_ERR_CUDA, std::string("ps_exclusive_scan_u32_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    scratch = static_cast<uint64_t*>(p);
-    g_noalloc_scratch_addr[dev].store(scratch, std::memory_order_release);
-  }
+  uint64_t* scratch = nullptr;
+  uint32_t* err = nullptr;
+  const int rc = noalloc_addrs("ps_exclusive_scan_u32_noalloc", &scratch, &err);
+  if (rc != PS_OK) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // the previous call left its ticket and tile flags behind: clear what this
   // call's tiles read
   PS_CUDA(cudaMemsetAsync(scratch, 0, scan_scratch_bytes(n), st));
-  k_exclusive_scan_u32<<<(unsigned)scan_num_tiles(n), SCAN_THREADS, 0, st>>>(d_in, d_out, n, scratch,
-                                                                             reinterpret_cast<uint32_t*>(scratch) + 1);
+  k_exclusive_scan_u32<<<(unsigned)scan_num_tiles(n), SCAN_THREADS, 0, st>>>(d_in, d_out, n, scratch, err);
   PS_CUDA(cudaGetLastError());
+  return PS_OK;
+}
+
+extern "C" int ps_exclusive_scan_u32_noalloc_status(void* stream, uint32_t* device_error) {
+  if (device_error == nullptr) return fail(PS_ERR_INVALID, "ps_exclusive_scan_u32_noalloc_status: null device_error");
+  uint64_t* scratch = nullptr;
+  uint32_t* err = nullptr;
+  const int rc = noalloc_addrs("ps_exclusive_scan_u32_noalloc_status", &scratch, &err);
+  if (rc != PS_OK) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  uint32_t word = 0;
+  PS_CUDA(cudaMemcpyAsync(&word, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  PS_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
+  PS_CUDA(cudaStreamSynchronize(st));
+  *device_error = word;
   return PS_OK;
 }

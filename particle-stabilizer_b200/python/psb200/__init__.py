@@ -27,7 +27,7 @@ EXPORTED = (
     "ps_grid_get", "ps_buckets_get", "ps_last_launch_count", "ps_destroy", "ps_simulate",
     "ps_exclusive_scan_scratch_bytes", "ps_exclusive_scan_u32", "ps_read_csv", "ps_write_csv", "ps_read_obj",
     "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "ps_forward_checkpointed",
-    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_autotune", "ps_set_contact_kernel", "ps_get_contact_kernel", "ps_set_neighbor_lists", "ps_list_stats", "ps_tune_neighbor_lists",
+    "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_exclusive_scan_u32_noalloc_status", "ps_autotune", "ps_set_contact_kernel", "ps_get_contact_kernel", "ps_set_neighbor_lists", "ps_list_stats", "ps_tune_neighbor_lists",
     "ps_resolve_overlaps", "ps_overlap_stats",
     "ps_write_obj_spheres", "runSimulateCUDA",
 )
@@ -111,6 +111,7 @@ def lib() -> C.CDLL:
         L.ps_forward_checkpointed.argtypes = [C.c_void_p, C.c_int64, C.c_int64]
         L.ps_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ps_exclusive_scan_u32_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        L.ps_exclusive_scan_u32_noalloc_status.argtypes = [C.c_void_p, C.POINTER(C.c_uint32)]
         L.ps_set_neighbor_lists.argtypes = [C.c_void_p, C.c_double, C.c_int32]
         L.ps_list_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ps_tune_neighbor_lists.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
@@ -367,6 +368,15 @@ def exclusive_scan_u32_noalloc(d_in: int, d_out: int, n: int, stream: int = 0) -
     allocation, using the library's fixed scratch array (n <= SCAN_NOALLOC_MAX_N)."""
     _check(lib().ps_exclusive_scan_u32_noalloc(C.c_void_p(d_in), C.c_void_p(d_out), int(n), C.c_void_p(stream)),
            "ps_exclusive_scan_u32_noalloc")
+
+
+def exclusive_scan_u32_noalloc_status(stream: int = 0) -> int:
+    """ps_exclusive_scan_u32_noalloc_status: the device error bits of the
+    no-allocation scans since the last query (0 = all complete), cleared."""
+    w = C.c_uint32()
+    _check(lib().ps_exclusive_scan_u32_noalloc_status(C.c_void_p(stream), C.byref(w)),
+           "ps_exclusive_scan_u32_noalloc_status")
+    return int(w.value)
 
 
 def exclusive_scan_scratch_bytes(n: int) -> int:

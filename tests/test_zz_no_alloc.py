@@ -8,7 +8,9 @@ from cudaMalloc.
 Checked through the C ABI against ps_exclusive_scan_u32 (which takes
 caller-provided scratch), bit for bit since the values are integers, on two
 calls in a row so the second call runs on the scratch the first one left
-behind.  This file is collected last; it also passes run alone.
+behind; the device error word that ps_exclusive_scan_u32_noalloc_status
+reports must stay zero (no look-back wait gave up).  This file is collected
+last; it also passes run alone.
 """
 import numpy as np
 import pytest
@@ -31,6 +33,7 @@ def test_noalloc_scan_equals_scan_on_consecutive_calls(need_gpu):
     import torch
 
     rng = np.random.default_rng(7)
+    assert psb200.exclusive_scan_u32_noalloc_status() == 0
     # a large call first, then a smaller one that reuses the stale scratch,
     # then one at the capacity limit
     for n in (3_000_017, 70_001, psb200.SCAN_NOALLOC_MAX_N):
@@ -48,6 +51,7 @@ def test_noalloc_scan_equals_scan_on_consecutive_calls(need_gpu):
         psb200.exclusive_scan_u32_noalloc(d_in.data_ptr(), d_in.data_ptr(), n, 0)
         torch.cuda.synchronize()
         assert np.array_equal(d_in.cpu().numpy().view(np.uint32), want), n
+        assert psb200.exclusive_scan_u32_noalloc_status() == 0, n
         del d_in, d_out
 
 
