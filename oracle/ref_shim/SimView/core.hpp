@@ -26,4 +26,8 @@ using Object_t = std::shared_ptr<Object>;
 struct Sphere : Primitive {};
 using Sphere_t = std::shared_ptr<Sphere>;
 }  // namespace model
+namespace app {
+struct ViewerGUIApp;  // named by Visualization.hpp only; never defined or used
+using ViewerGUIApp_t = std::shared_ptr<ViewerGUIApp>;
+}  // namespace app
 }  // namespace simview

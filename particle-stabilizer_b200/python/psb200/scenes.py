@@ -259,13 +259,16 @@ def box_mesh_scene(n: int = 120, seed: int = 41) -> Scene:
                  tri=box_container(), name="box_mesh")
 
 
-def funnel_wall_scene(n: int = 2000, seed: int = 7, coarse: bool = True) -> Scene:
+def funnel_wall_scene(n: int = 2000, seed: int = 7, coarse: bool = True, z_max: float = 1.05,
+                      widen: bool = True) -> Scene:
     """Spheres (r 0.003) on rings just inside the funnel's cone wall at
-    heights 0.45..0.9, pressing outward, plus some above the rim: every
-    step has triangle contacts.  A coarse funnel keeps the all-pairs oracle fast."""
+    heights 0.45..z_max, pressing outward (with the default z_max some start
+    above the rim): every step has triangle contacts.  A coarse funnel keeps
+    the all-pairs oracle fast.  With z_max below 1 every centre lies inside
+    the mesh AABB, the grid domain of the reference's CUDA path."""
     rng = np.random.default_rng(seed)
     tri = funnel_triangles(64, 12, 3, 2) if coarse else funnel_triangles()
-    z = rng.uniform(0.45, 1.05, size=n)
+    z = rng.uniform(0.45, z_max, size=n)
     t = np.clip((1.0 - z) / 0.7, 0.0, 1.0)
     wall_r = 0.5 + (0.08 - 0.5) * t
     rad = wall_r - rng.uniform(0.0, 0.004, size=n)
@@ -274,8 +277,8 @@ def funnel_wall_scene(n: int = 2000, seed: int = 7, coarse: bool = True) -> Scen
     vel = np.stack([0.3 * np.cos(th), 0.3 * np.sin(th), rng.normal(0, 0.1, n)], 1)
     st = _state(pos, vel, np.full(n, 0.003), 1000.0)
     e = (0.6,) * 6
-    return Scene(st, (-0.5, -0.5, 0.0), (0.5, 0.5, 1.0), (0, 0, -9.8), e, 2e-2, 0.5, 5e-6, tri=tri, widen_domain=1,
-                 name="funnel_wall")
+    return Scene(st, (-0.5, -0.5, 0.0), (0.5, 0.5, 1.0), (0, 0, -9.8), e, 2e-2, 0.5, 5e-6, tri=tri,
+                 widen_domain=1 if widen else 0, name="funnel_wall")
 
 
 def write_obj(path: str, tri: np.ndarray) -> None:

@@ -63,10 +63,24 @@ def test_oracle_cpu_semantics_mesh_bitexact():
 CUDA_FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "ref_cuda_*.npz")))
 
 
+def fixture_scene(g):
+    """Scene of a reference CUDA fixture: a box, or a triangle container read
+    from OBJ (grid domain = the mesh AABB, the reference's edge pick)."""
+    sc = box_scene(g["init"], g["box"], g["e_wall"], g["k"], g["es"], g["dt"])
+    if "tri" in g.files:
+        sc = sc.copy(tri=g["tri"], edge_quirk=1, widen_domain=0)
+    return sc
+
+
+def test_reference_cuda_fixtures_cover_both_containers():
+    names = {os.path.basename(p) for p in CUDA_FIXTURES}
+    assert {"ref_cuda_lattice.npz", "ref_cuda_pile.npz", "ref_cuda_mesh_box.npz", "ref_cuda_mesh_funnel.npz"} <= names
+
+
 @pytest.mark.parametrize("path", CUDA_FIXTURES, ids=[os.path.basename(p) for p in CUDA_FIXTURES])
 def test_oracle_cuda_semantics_vs_reference_cuda(path):
     g = np.load(path)
-    sc = box_scene(g["init"], g["box"], g["e_wall"], g["k"], g["es"], g["dt"])
+    sc = fixture_scene(g)
     og = O.grid_for(sc)
     assert tuple(og.nb) == tuple(g["nb"]) and og.interval == float(g["interval"])
     for i, s in enumerate(g["steps"]):
@@ -241,3 +255,35 @@ def test_fp32_run_tracks_fp64_run(name):
     vs = np.abs(b[:, 3:6]).max()
     assert np.abs(a[:, :3] - b[:, :3]).max() < pos_tol * L
     assert np.abs(a[:, 3:6] - b[:, 3:6]).max() < vel_tol * vs
+
+
+# ---- 4. the forward-mode gradient oracle against central differences ---------
+def test_dual_oracle_vs_central_fd_on_contact_pile():
+    """oracle/ps_oracle_dual.c (forward-mode FP64, the reference gradient of
+    the GPU adjoint) against FP64 central differences of the oracle's own
+    forward run, on the 1,024-sphere contact pile over 400 steps: each
+    non-zero parameter derivative of the settling loss within 1e-3
+    relative; the contact spring, sphere restitution and floor restitution
+    derivatives are non-zero."""
+    import psb200
+
+    sc = scenes.pile(1024, seed=3, k_spring=1.0)
+    steps = 400
+    st, tang = O.run_dual(sc, steps, np.eye(8), np.zeros((8, sc.n, 6)))
+    _, gl = psb200.height_loss(st)
+    fm = np.array([np.sum(gl * tang[d]) for d in range(8)])
+    theta = np.array([sc.k_spring, sc.e_sphere, *sc.e_wall])
+    for p in range(8):
+        h = 1e-6 * max(1.0, abs(theta[p]))
+        tp, tm = theta.copy(), theta.copy()
+        tp[p] += h
+        tm[p] -= h
+        lp = psb200.height_loss(O.run(sc.copy(k_spring=tp[0], e_sphere=tp[1], e_wall=tuple(tp[2:])), steps))[0]
+        lm = psb200.height_loss(O.run(sc.copy(k_spring=tm[0], e_sphere=tm[1], e_wall=tuple(tm[2:])), steps))[0]
+        fd = (lp - lm) / (2 * h)
+        if p in (0, 1, 2):
+            assert fd != 0.0
+        if fd == 0.0:
+            assert fm[p] == 0.0
+        else:
+            assert abs(fm[p] - fd) <= 1e-3 * abs(fd), (p, fm[p], fd)

@@ -64,6 +64,108 @@ def test_counts_offsets_sets_equal_reference(need_gpu, make, steps):
 
 
 @needs_ref
+def test_1000_step_trajectories_within_reference_run_to_run_spread(need_gpu):
+    """1,000 steps of a stable contact-rich pile (4,096 polydisperse spheres,
+    spring 1) against five runs of the reference's own CUDA build, which
+    sums contact kicks with FP64 atomics in an order that changes from run
+    to run.
+
+    Tolerances, per particle and component (positions and velocities):
+      FP64: within 10x the reference's own run-to-run spread of that
+            particle and component (largest difference between two of its
+            five runs), plus 1e-12 of the component's largest magnitude (for
+            particles the reference always sums in the same order);
+      FP32: within 2e-4 of the largest box edge in position and 3e-2 of the
+            largest speed component in velocity, of every reference run and
+            of the FP64 oracle (measured 7e-5 / 1e-2 on this scene class)."""
+    sc = scenes.pile(4096, seed=21, k_spring=1.0)
+    steps, runs = 1000, 5
+    r = O.ref_cuda()
+    refs = []
+    for _ in range(runs):
+        h = r.create(sc)
+        try:
+            r.step(h, steps)
+            refs.append(r.state(h, sc.n))
+        finally:
+            r.destroy(h)
+    R = np.stack(refs)
+    assert np.isfinite(R).all()
+    spread = R.max(axis=0) - R.min(axis=0)       # (n, 8): per particle and component
+    scale = np.abs(R).max(axis=(0, 1)) + 1e-300  # per component
+    with psb200.Simulation(sc, "f64") as sim:
+        sim.set_state()
+        sim.step(steps)
+        ours64 = sim.get_state()
+    with psb200.Simulation(sc, "f32") as sim:
+        sim.set_state()
+        sim.step(steps)
+        ours32 = sim.get_state()
+    assert np.array_equal(ours64, O.run(sc, steps, "f64"))
+    dev64 = np.abs(ours64[None] - R).max(axis=0)
+    tol64 = 10.0 * spread + 1e-12 * scale
+    assert np.all(dev64[:, :6] <= tol64[:, :6]), float((dev64[:, :6] / tol64[:, :6]).max())
+    edge = max(b - a for a, b in zip(sc.box_min, sc.box_max))
+    vmax = np.abs(R[:, :, 3:6]).max()
+    for other in [*refs, ours64]:
+        assert np.abs(ours32[:, :3] - other[:, :3]).max() <= 2e-4 * edge
+        assert np.abs(ours32[:, 3:6] - other[:, 3:6]).max() <= 3e-2 * vmax
+    moved = np.abs(R[0, :, :3] - sc.state[:, :3]).max()
+    print(f"\n1,000 steps, 4,096-sphere pile: reference run-to-run spread max {spread[:, :3].max():.2e} (pos) "
+          f"{spread[:, 3:6].max():.2e} (vel); FP64 deviation max {dev64[:, :3].max():.2e} / "
+          f"{dev64[:, 3:6].max():.2e}; FP32 deviation max {np.abs(ours32[:, :3] - R[0, :, :3]).max():.2e} / "
+          f"{np.abs(ours32[:, 3:6] - R[0, :, 3:6]).max():.2e}; largest displacement {moved:.2e}")
+
+
+MESH_SCENES = {
+    "box": lambda: scenes.box_mesh_scene(),
+    "funnel": lambda: scenes.funnel_wall_scene(600, seed=17, z_max=0.95, widen=False),
+}
+
+
+@needs_ref
+@pytest.mark.parametrize("name", sorted(MESH_SCENES))
+@pytest.mark.parametrize("steps", [1, 6, 30])
+def test_triangle_container_equals_reference_cuda(need_gpu, tmp_path, name, steps):
+    """The triangle container against the reference's own CUDA mesh path
+    (PolygonContainerCUDA::resolveCollisions, PolygonContainerCUDA.cpp:
+    130-226, kernels PolygonContainerCUDA_kernels.cu:114-294), read from the
+    same OBJ file: a closed triangulated box whose outer spheres touch its
+    walls and floor, and spheres pressing on the cone wall of a coarse
+    funnel.  Every centre starts inside the mesh AABB, the reference's grid
+    domain.  Counts and offsets are compared exactly, bucket members as
+    sets, states within FP64 rounding of the reference's atomic sums."""
+    sc = MESH_SCENES[name]()
+    obj = str(tmp_path / "container.obj")
+    scenes.write_obj(obj, sc.tri)
+    r = O.ref_cuda()
+    h = r.create(sc, obj)
+    try:
+        r.step(h, steps)
+        ref_state = r.state(h, sc.n)
+        og = O.grid_for(sc)
+        rc, ro, rb = ref_buckets(r, h, sc.n, og.n_cells)
+    finally:
+        r.destroy(h)
+    with psb200.Simulation(sc, "f64") as sim:
+        sim.set_state()
+        sim.step(steps)
+        counts, offsets, order = sim.buckets()
+        st = sim.get_state()
+    assert np.array_equal(counts, rc)
+    assert np.array_equal(offsets, ro)
+    for c in np.nonzero(rc)[0]:
+        a, b = ro[c], ro[c] + rc[c]
+        assert np.array_equal(np.sort(rb[a:b]), order[a:b].astype(np.int64))
+    # the container acted: the same steps in a loose box differ
+    loose = sc.copy(tri=None, box_min=(-1, -1, -1), box_max=(1, 1, 2))
+    assert np.any(O.run(loose, steps, "f64") != ref_state)
+    scale = np.abs(ref_state).max(axis=0) + 1e-300
+    rel = (np.abs(st - ref_state) / scale).max()
+    assert rel < 1e-12, rel
+
+
+@needs_ref
 def test_head_to_head_with_reference_cuda_at_1m_spheres(need_gpu):
     """Throughput against the reference's own CUDA build on the same B200:
     the 1,048,576-sphere scene with a spring the scheme integrates stably
