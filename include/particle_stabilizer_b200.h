@@ -196,8 +196,8 @@ int ps_backward(ps_sim* sim, const double* dl_dstate, ps_grad* grads, double* dl
  * and equal to the oracle's with that cell size, but not bit-equal to runs
  * with the previous grid.  A recorded ps_forward_checkpointed is dropped.
  * Then, on the chosen grid and L, it times the four contact kernels
- * (PS_WALK_LANE with 256 threads per CTA, PS_WALK_WARP with 128, 256 and
- * 512) and keeps the fastest; they give identical results.
+ * (PS_WALK_LANE with 128, 256 and 512 threads per CTA, PS_WALK_WARP with
+ * 256) and keeps the fastest; they give identical results.
  * Allocates device memory (grids, graphs, one state copy). */
 /* ---- neighbour-list mode (no counterpart in the reference, which rebuilds
  * its grid every step, ParticleModelCUDA.cpp:115-155) ----
@@ -237,8 +237,8 @@ typedef struct ps_tune_result {
   int32_t contact_walk;      /* chosen contact kernel: PS_WALK_LANE / PS_WALK_WARP */
   int32_t contact_block;     /* and its threads per CTA                           */
   double contact_ms[4];      /* ms per step, with the chosen f and L, of the      */
-                             /* contact kernels LANE/256, WARP/128, WARP/256,     */
-                             /* WARP/512                                          */
+                             /* contact kernels LANE/128, LANE/256, LANE/512,     */
+                             /* WARP/256                                          */
 } ps_tune_result;
 int ps_autotune(ps_sim* sim, int64_t trial_steps, const double* cell_factors, int32_t n_factors,
                 const int64_t* graph_blocks, int32_t n_blocks, double* ms_table, ps_tune_result* out);
@@ -247,13 +247,14 @@ int ps_autotune(ps_sim* sim, int64_t trial_steps, const double* cell_factors, in
  * particle, one per neighbour cell (ParticleModel_kernels.cu:136-201,
  * launch :342-372); there is nothing to choose there.  PS_WALK_LANE: each
  * thread loops over its own nine slot ranges (the 27 cells as nine
- * (x, y) columns of three z-cells), 256 threads per CTA.  PS_WALK_WARP:
- * each warp reads the union of its 32 spheres' candidates in a neighbour
- * column with coalesced loads and hands them to the lanes by register
- * shuffle; 128, 256 or 512 threads per CTA.  Every variant applies the same
- * candidates in the same order, so results are bit-identical; only the
- * speed differs.  The default is PS_WALK_WARP with 256 threads.  Changing
- * it drops the captured step graphs. */
+ * (x, y) columns of three z-cells), 128, 256 or 512 threads per CTA.
+ * PS_WALK_WARP: each warp reads the union of its 32 spheres' candidates in
+ * a neighbour column with coalesced loads and hands them to the lanes by
+ * register shuffle; 256 threads per CTA (measured slower than the lane walk
+ * on every scene tried; kept as a tuner candidate).  Every variant applies
+ * the same candidates in the same order, so results are bit-identical;
+ * only the speed differs.  The default is PS_WALK_LANE with 256 threads.
+ * Changing it drops the captured step graphs. */
 #define PS_WALK_LANE 0
 #define PS_WALK_WARP 1
 int ps_set_contact_kernel(ps_sim* sim, int32_t walk, int32_t block);

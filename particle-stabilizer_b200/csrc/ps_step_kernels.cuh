@@ -389,15 +389,17 @@ __device__ __forceinline__ vec4_t<T> shfl4(const vec4_t<T>& v, int src) {
 // bit-identical to it.
 //
 // Loads per lane and window, and columns whose first window is in flight
-// while the current column is walked.  FP64 holds half as many: a double4
-// window per lane is 8 registers.
+// while the current column is walked.
+// Measured on the 1M-sphere scenes (FP32 contact kernel, 256 threads): one
+// window of 32 and one column ahead 76.5 us; two windows and two ahead
+// 102.7 us; one window three ahead 82.5 us; the lane walk 57.7 us.
 template <class T>
 __host__ __device__ constexpr int walk_window() {
-  return sizeof(T) == 4 ? 2 : 1;
+  return 1;
 }
 template <class T>
 __host__ __device__ constexpr int walk_ahead() {
-  return sizeof(T) == 4 ? 2 : 1;
+  return 1;
 }
 
 template <class T>

@@ -68,7 +68,7 @@ class TuneResult(C.Structure):
 
 WALK_LANE, WALK_WARP = 0, 1
 # contact kernel variants in the order of TuneResult.contact_ms: (walk, threads per CTA)
-CONTACT_KERNELS = ((WALK_LANE, 256), (WALK_WARP, 128), (WALK_WARP, 256), (WALK_WARP, 512))
+CONTACT_KERNELS = ((WALK_LANE, 128), (WALK_LANE, 256), (WALK_LANE, 512), (WALK_WARP, 256))
 
 
 class PSError(RuntimeError):
@@ -294,8 +294,8 @@ class Simulation:
                 "contact_ms": [float(x) for x in res.contact_ms], "contact_kernels": list(CONTACT_KERNELS)}
 
     def set_contact_kernel(self, walk: int, block: int) -> None:
-        """ps_set_contact_kernel: WALK_LANE with 256 threads per CTA, or
-        WALK_WARP with 128, 256 or 512 (identical results)."""
+        """ps_set_contact_kernel: WALK_LANE with 128, 256 or 512 threads per
+        CTA, or WALK_WARP with 256 (identical results)."""
         _check(lib().ps_set_contact_kernel(self.h, int(walk), int(block)), "ps_set_contact_kernel")
 
     def contact_kernel(self) -> tuple[int, int]:

@@ -43,8 +43,8 @@ def test_autotune_choice_restores_state_and_keeps_parity(need_gpu):
 
 @pytest.mark.parametrize("precision", ["f32", "f64"])
 def test_every_contact_kernel_gives_the_same_states(need_gpu, precision):
-    """The four contact kernels (per-lane walk with 256 threads per CTA,
-    warp walk with 128, 256 and 512) on a batch of a dense pile, a sparse
+    """The four contact kernels (per-lane walk with 128, 256 and 512 threads
+    per CTA, warp walk with 256) on a batch of a dense pile, a sparse
     lattice and a triangle container: states bit-identical to each other
     and to the oracle after 40 steps."""
     batch = [scenes.pile(1500, seed=41, k_spring=1.0), scenes.lattice_c1(side=10), scenes.box_mesh_scene()]
@@ -77,6 +77,6 @@ def test_autotune_rejects_bad_arguments(need_gpu):
         with pytest.raises(psb200.PSError, match="bad argument"):
             sim.autotune(trial_steps=0)
         with pytest.raises(psb200.PSError, match="walk/block"):
-            sim.set_contact_kernel(psb200.WALK_LANE, 128)
+            sim.set_contact_kernel(psb200.WALK_WARP, 128)
         with pytest.raises(psb200.PSError, match="walk/block"):
-            sim.set_contact_kernel(psb200.WALK_WARP, 1024)
+            sim.set_contact_kernel(psb200.WALK_LANE, 1024)
