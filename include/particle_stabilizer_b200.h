@@ -99,7 +99,8 @@ const char* ps_last_error(void);
  * runSimulateCUDA: ParticleModelCUDA ctor + container ctor + initBuckets
  * (PhysicsEngineCUDA.cpp:98-117, ParticleModelCUDA.cpp:4-52,62-113).
  * Several scenes advance together in every launch (batched execution).
- * The grid's r_max is taken from the first ps_set_state. */
+ * The grid's r_max is taken from the first ps_set_state.  At most
+ * 2^31 - 65 particles over all scenes (PS_ERR_INVALID beyond). */
 int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t precision, int32_t device, ps_sim** out);
 
 /* Upload host state, scenes concatenated in order (replaces the H2D copy

@@ -1241,7 +1241,7 @@ extern "C" int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t 
   }
   s->n_total = s->pbase[n_scenes];
   s->multi = n_scenes > 1;
-  if (s->n_total >= (int64_t)UINT32_MAX - 1) {
+  if (s->n_total >= (int64_t)SLOT_ALONE - 64) {  // slot tags and union walks stay below 2^31
     delete s;
     return fail(PS_ERR_INVALID, "ps_create: too many particles");
   }

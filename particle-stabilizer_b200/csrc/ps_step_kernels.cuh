@@ -217,10 +217,18 @@ __global__ void __launch_bounds__(STEP_THREADS) k_begin(StepBufs<T> b, ScenePara
 
 constexpr int MOVE_PER_THREAD = 4;
 
+// slot[p] of a sphere alone in its cell: its final position, tagged.  (The
+// scan's offsets and positions are below 2^31: ps_create caps the particle
+// count there.)
+constexpr uint32_t SLOT_ALONE = 0x80000000u;
+
 // slot = --count[c], a distinct slot of the cell for every member (the
 // decrements bring every count back to zero for the next step);
-// tmp[offset[c] + slot] = orig, and the slot is kept for k_rank_move.  The
-// tile totals are cleared for the next count.
+// tmp[offset[c] + slot] = orig, and the slot is kept for k_rank_move.  A
+// sphere alone in its cell (offset[c + 1] == offset[c] + 1, most cells at a
+// few tenths of a sphere per cell) keeps its final position offset[c]
+// instead, tagged SLOT_ALONE, so k_rank_move moves it without reading the
+// offsets again or ranking.  The tile totals are cleared for the next count.
 // MOVE_PER_THREAD particles per thread, strided by the block so that every
 // load instruction stays coalesced; all loads are issued before the stores.
 // Block `blk` of the scatter (COH: see ld_ro).
@@ -232,7 +240,8 @@ __device__ __forceinline__ void scatter_block(uint32_t blk, const uint32_t* __re
   const uint32_t t = blk * STEP_THREADS + threadIdx.x;
   if (t < n_tiles) tile_sum[t] = 0u;
   const uint32_t base = blk * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
-  uint32_t c[MOVE_PER_THREAD], sl[MOVE_PER_THREAD], o[MOVE_PER_THREAD], off[MOVE_PER_THREAD];
+  uint32_t c[MOVE_PER_THREAD], sl[MOVE_PER_THREAD], o[MOVE_PER_THREAD], off[MOVE_PER_THREAD],
+      nxt[MOVE_PER_THREAD];
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     const uint32_t p = base + k * STEP_THREADS;
@@ -243,13 +252,14 @@ __device__ __forceinline__ void scatter_block(uint32_t blk, const uint32_t* __re
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     const bool in = (base + k * STEP_THREADS) < n;
     off[k] = in ? ld_ro<COH>(offset + c[k]) : 0u;
+    nxt[k] = in ? ld_ro<COH>(offset + c[k] + 1) : 0u;
     sl[k] = in ? atomicSub(count + c[k], 1u) - 1u : 0u;
   }
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     if (base + k * STEP_THREADS < n) {
       tmp[off[k] + sl[k]] = o[k];
-      slot[base + k * STEP_THREADS] = sl[k];
+      slot[base + k * STEP_THREADS] = nxt[k] - off[k] == 1u ? (off[k] | SLOT_ALONE) : sl[k];
     }
   }
 }
@@ -266,13 +276,15 @@ __global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __rest
 
 // Canonical position = offset[c] + #{members of c with a smaller orig id};
 // moves the integrated state (P1, V1) there as (P0, V0) with its orig id.
+// A sphere alone in its cell has its position from k_scatter (SLOT_ALONE).
 template <class T, bool COH>
 __device__ __forceinline__ void rank_move_block(uint32_t blk, const StepBufs<T>& b) {
   const uint32_t base = blk * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
-  // Loads in three dependent rounds, each issued for all MOVE_PER_THREAD
+  // Loads in dependent rounds, each issued for all MOVE_PER_THREAD
   // particles before any store (the stores could alias them as far as the
   // compiler knows, which would otherwise serialise the rounds per particle):
-  // cell, slot and the moved state; the cell's range; the member's orig id.
+  // cell, slot and the moved state; the cell's range (shared cells only);
+  // the member's orig id.
   uint32_t c[MOVE_PER_THREAD], sl[MOVE_PER_THREAD], start[MOVE_PER_THREAD], end[MOVE_PER_THREAD],
       o[MOVE_PER_THREAD];
   vec4_t<T> P[MOVE_PER_THREAD], V[MOVE_PER_THREAD];
@@ -289,9 +301,10 @@ __device__ __forceinline__ void rank_move_block(uint32_t blk, const StepBufs<T>&
   }
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
-    const bool in = base + k * STEP_THREADS < b.n;
-    start[k] = in ? ld_ro<COH>(b.offset + c[k]) : 0u;
-    end[k] = in ? ld_ro<COH>(b.offset + c[k] + 1) : 0u;
+    const bool shared = base + k * STEP_THREADS < b.n && !(sl[k] & SLOT_ALONE);
+    start[k] = shared ? ld_ro<COH>(b.offset + c[k]) : (sl[k] & ~SLOT_ALONE);
+    end[k] = shared ? ld_ro<COH>(b.offset + c[k] + 1) : start[k] + 1u;
+    if (!shared) sl[k] = 0u;
   }
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k)
@@ -300,7 +313,8 @@ __device__ __forceinline__ void rank_move_block(uint32_t blk, const StepBufs<T>&
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     if (base + k * STEP_THREADS >= b.n) continue;
     uint32_t rank = 0;
-    for (uint32_t s = start[k]; s < end[k]; ++s) rank += (b.tmp[s] < o[k]) ? 1u : 0u;
+    if (end[k] - start[k] > 1u)
+      for (uint32_t s = start[k]; s < end[k]; ++s) rank += (b.tmp[s] < o[k]) ? 1u : 0u;
     const uint32_t d = start[k] + rank;
     b.P0[d] = P[k];
     b.V0[d] = V[k];
