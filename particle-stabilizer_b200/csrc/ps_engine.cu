@@ -1321,8 +1321,13 @@ extern "C" int ps_set_state(ps_sim* s, const double* aos, int64_t n_total) {
     k_upload<double><<<g, STEP_THREADS, 0, s->stream>>>(s->staging, static_cast<vec4_t<double>*>(s->P0),
                                                         static_cast<vec4_t<double>*>(s->V1), s->orig, (uint32_t)n_total);
   PS_CUDA(cudaGetLastError());
+  // Keep the state at rest in grid order, as every step leaves it: the
+  // first step after an upload (or after restoring a checkpoint saved now)
+  // then counts its cells in sorted order, one tile-total atomic per warp,
+  // instead of scattering them over every tile.
+  const int rc = regrid(s);
+  if (rc != PS_OK) return rc;
   PS_CUDA(cudaStreamSynchronize(s->stream));
-  s->grid_valid = false;
   return PS_OK;
 }
 
