@@ -523,11 +523,12 @@ __global__ void __launch_bounds__(BLOCK, contact_min_blocks<T, BLOCK>()) k_conta
   }
   const T ks = sp.k_spring, es = sp.e_sphere;
   if constexpr (WALK == WALK_LANE) {
-    // visit the nine ranges in canonical order
+    // visit the nine ranges in canonical order; only the own column (q = 4)
+    // holds the sphere itself
 #pragma unroll
     for (int q = 0; q < 9; ++q)
       for (uint32_t j = lo[q]; j < hi[q]; ++j) {
-        if (j == i) continue;
+        if (q == 4 && j == i) continue;
         contact_one<T>(b.V0, j, P, Vi, ld4<T>(b.P0 + j), ks, es, vx, vy, vz);
       }
   } else {
