@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_adj_contacts(StepBufs<T> b, Ad
   #pragma unroll
     for (int q = 0; q < 9; ++q)
       for (uint32_t j = lo[q]; j < hi[q]; ++j) {
-        if (j == i) continue;
+        if (q == 4 && j == i) continue;  // only the own column holds the sphere itself
         const vec4_t<T> Pj = ld4<T>(b.P0 + j);
         if (!pair_active<T>(P, Pj)) continue;
         const vec4_t<T> Vj = b.V0[j];
