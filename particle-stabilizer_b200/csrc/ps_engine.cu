@@ -116,8 +116,6 @@ struct ps_sim {
 
   std::map<int64_t, cudaGraphExec_t> graphs;
   int64_t graph_block = 200;  // steps per captured CUDA graph (ps_autotune may change it)
-  bool stream_scan = false;   // k_scan_stream set up for this device (dynamic shared memory granted)
-  int num_sms = 0;
   int32_t walk = WALK_LANE;   // neighbour walk of the contact kernel (WALK_LANE / WALK_WARP)
   int32_t contact_block = 256;  // threads per CTA of the contact kernel (WALK_LANE: 128, 256, 512; WALK_WARP: 256)
   int64_t last_launches = 0;
@@ -156,21 +154,6 @@ int64_t n_scan(const ps_sim* s) { return s->c_total + 1; }
 // Launch with programmatic stream serialization: the kernel may start while
 // its predecessor on the stream drains; it waits (griddepcontrol.wait, a
 // no-op for a normal launch) before reading anything the predecessor wrote.
-template <typename... KArgs, typename... Args>
-void pdl_launch_smem(void (*k)(KArgs...), unsigned g, unsigned blk, size_t smem, cudaStream_t st, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(g);
-  cfg.blockDim = dim3(blk);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k, args...);
-}
-
 template <typename... KArgs, typename... Args>
 void pdl_launch(void (*k)(KArgs...), unsigned g, unsigned blk, cudaStream_t st, Args... args) {
   cudaLaunchConfig_t cfg = {};
@@ -267,28 +250,6 @@ ContactLaunch<T, MULTI, MESH, FUSED> contacts_kernel(const ps_sim* s) {
   return c;
 }
 
-// The step's scan of the cell counts into `out` (the tile totals are in
-// s->tile_sum): the streaming kernel when the simulation could set it up,
-// else one CTA per tile.
-void launch_step_scan(ps_sim* s, uint32_t* out, cudaStream_t st, bool pdl) {
-  const int64_t nsc = n_scan(s);
-  const int64_t tiles = scan_num_tiles(nsc);
-  if (s->stream_scan) {
-    const unsigned g = (unsigned)std::min<int64_t>(tiles, (int64_t)s->num_sms * SSCAN_CTAS_PER_SM);
-    if (pdl)
-      pdl_launch_smem(k_scan_stream, g, SCAN_THREADS, SSCAN_SMEM, st, (const uint32_t*)s->count, out, nsc,
-                      (const uint32_t*)s->tile_sum, s->err);
-    else
-      k_scan_stream<<<g, SCAN_THREADS, SSCAN_SMEM, st>>>(s->count, out, nsc, s->tile_sum, s->err);
-  } else {
-    if (pdl)
-      pdl_launch(k_scan_with_tile_sums, (unsigned)tiles, SCAN_THREADS, st, (const uint32_t*)s->count, out, nsc,
-                 (const uint32_t*)s->tile_sum);
-    else
-      k_scan_with_tile_sums<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(s->count, out, nsc, s->tile_sum);
-  }
-}
-
 // ---- the launch sequence -----------------------------------------------------
 template <class T, bool MULTI, bool MESH>
 int64_t enqueue_steps(ps_sim* s, int64_t steps) {
@@ -305,7 +266,8 @@ int64_t enqueue_steps(ps_sim* s, int64_t steps) {
   pdl_launch(k_begin<T, MULTI, MESH, true>, gb, STEP_THREADS, st, b, sp0, mv);
   ++launches;
   for (int64_t k = 0; k < steps; ++k) {
-    launch_step_scan(s, s->offset, st, true);
+    pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, nsc,
+               (const uint32_t*)s->tile_sum);
     pdl_launch(k_scatter, move_blocks(s->n_total, b.n_tiles), STEP_THREADS, st, (const uint32_t*)s->cell, s->slot,
                (const uint32_t*)s->orig, (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles);
     pdl_launch(k_rank_move<T>, move_blocks(s->n_total, 0), STEP_THREADS, st, b);
@@ -346,7 +308,7 @@ void enqueue_steps_recorded(ps_sim* s, int64_t steps, std::vector<LaunchRecord>&
   post();
   for (int64_t k = 0; k < steps; ++k) {
     pre(PS_K_SCAN);
-    launch_step_scan(s, s->offset, st, false);
+    k_scan_with_tile_sums<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->tile_sum);
     post();
     pre(PS_K_SCATTER);
     k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
@@ -429,7 +391,8 @@ cudaError_t enqueue_steps_list(ps_sim* s, int64_t steps) {
   cudaMemsetAsync(s->count, 0, sizeof(uint32_t) * (size_t)nsc, st);
   cudaMemsetAsync(s->tile_sum, 0, sizeof(uint32_t) * (size_t)b.n_tiles, st);
   pdl_launch(k_begin<T, MULTI, MESH, true>, gp, STEP_THREADS, st, b, sp0, mv);
-  launch_step_scan(s, s->offset, st, true);
+  pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, nsc,
+             (const uint32_t*)s->tile_sum);
   pdl_launch(k_scatter, gm0, STEP_THREADS, st, (const uint32_t*)s->cell, s->slot, (const uint32_t*)s->orig,
              (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles);
   pdl_launch(k_rank_move<T>, gm1, STEP_THREADS, st, b);
@@ -506,7 +469,8 @@ void enqueue_regrid(ps_sim* s) {
   const unsigned gp = blocks_for(s->n_total);
   cudaStream_t st = s->stream;
   k_begin<T, MULTI, false, false><<<gb, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
-  launch_step_scan(s, s->offset, st, false);
+  k_scan_with_tile_sums<<<(unsigned)scan_num_tiles(n_scan(s)), SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s),
+                                                                                     s->tile_sum);
   k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
                                                                        s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
   k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
@@ -1123,7 +1087,8 @@ int enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes, 
     b.tape_o = row.o;
     uint32_t* off_k = offs + offs_stride * (size_t)k;
     b.offset = off_k;
-    launch_step_scan(s, off_k, st, true);
+    pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, off_k, n_scan(s),
+               (const uint32_t*)s->tile_sum);
     pdl_launch(k_scatter, move_blocks(s->n_total, b.n_tiles), STEP_THREADS, st, (const uint32_t*)s->cell, s->slot,
                (const uint32_t*)s->orig, (const uint32_t*)off_k, s->tmp, s->count, (uint32_t)s->n_total,
                s->tile_sum, b.n_tiles);
@@ -1308,10 +1273,6 @@ extern "C" int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t 
   s->d_stats_out = reinterpret_cast<StatsPartial*>(p);
   std::vector<uint32_t> pb(n_scenes + 1);
   for (int sc = 0; sc <= n_scenes; ++sc) pb[sc] = (uint32_t)s->pbase[sc];
-  if (cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && s->num_sms > 0 &&
-      cudaFuncSetAttribute(k_scan_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SSCAN_SMEM) == cudaSuccess)
-    s->stream_scan = true;
-  cudaGetLastError();
   e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMemcpy(s->d_pbase, pb.data(), 4 * pb.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(s->err, 0, 256);

@@ -254,179 +254,4 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_with_tile_sums(const uint
   scan_tile_with_sums<false>(blockIdx.x, in, out, n, tile_sum);
 }
 
-// ---- streaming step scan (TMA bulk copies into shared memory) -------------
-// The step's scan with the tile totals already known, as k_scan_with_tile_sums,
-// but a fixed grid of SSCAN_CTAS_PER_SM CTAs per SM, each taking a contiguous
-// run of tiles and streaming them: the 32-KB count tiles are brought into
-// shared memory by cp.async.bulk (one thread issues, an mbarrier counts the
-// bytes in), SSCAN_STAGES tiles in flight per CTA, so a CTA scans one tile
-// while the next ones arrive.  Each run's first prefix is the sum of the tile
-// totals before it; from there the CTA carries its running total.  Results
-// are the same integers as the one-tile-per-CTA kernel.
-//
-// Every wait on a barrier is bounded (SSCAN_SPIN_LIMIT polls): a CTA whose
-// copy never completes records PS_DEVERR_SCAN_TIMEOUT, waits (bounded) for
-// its other copies in flight, and returns.  A run's last tile, when partial,
-// is read with plain loads (a bulk copy moves whole 16-byte units).
-constexpr int SSCAN_STAGES = 2;
-constexpr int SSCAN_CTAS_PER_SM = 2;
-constexpr uint32_t SSCAN_SPIN_LIMIT = 1u << 22;
-constexpr size_t SSCAN_SMEM = (size_t)SSCAN_STAGES * SCAN_TILE * sizeof(uint32_t);
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n"
-      " .reg .pred p;\n"
-      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n"
-      "}\n"
-      : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return done != 0u;
-}
-// Bulk copy global -> this CTA's shared memory, completion counted on `bar`.
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_stream(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                                                             int64_t n, const uint32_t* __restrict__ tile_sum,
-                                                             uint32_t* err) {
-  extern __shared__ __align__(128) unsigned char sscan_raw[];
-  uint32_t* stage = reinterpret_cast<uint32_t*>(sscan_raw);  // SSCAN_STAGES tiles
-  __shared__ __align__(8) uint64_t bar[SSCAN_STAGES];
-  __shared__ uint32_t s_warp[SCAN_THREADS / 32];
-  __shared__ uint32_t s_red[SCAN_THREADS / 32];
-  constexpr int ROWS = SCAN_ITEMS / 4;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t n_tiles = scan_num_tiles(n);
-  const int64_t n_full = n / SCAN_TILE;  // tiles wholly inside [0, n): moved by bulk copy
-  const int64_t G = gridDim.x, per = n_tiles / G, rem = n_tiles % G;
-  const int64_t t0 = (int64_t)blockIdx.x * per + ((int64_t)blockIdx.x < rem ? (int64_t)blockIdx.x : rem);
-  const int64_t t1 = t0 + per + ((int64_t)blockIdx.x < rem ? 1 : 0);
-  if (tid == 0) {
-    for (int s = 0; s < SSCAN_STAGES; ++s) mbar_init(&bar[s], 1u);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  pdl_wait();
-  auto issue = [&](int64_t t, int s) {
-    if (t < t1 && t < n_full) {
-      mbar_expect_tx(&bar[s], (uint32_t)(SCAN_TILE * sizeof(uint32_t)));
-      bulk_load(stage + (size_t)s * SCAN_TILE, in + t * SCAN_TILE, (uint32_t)(SCAN_TILE * sizeof(uint32_t)), &bar[s]);
-    }
-  };
-  if (tid == 0)
-    for (int s = 0; s < SSCAN_STAGES; ++s) issue(t0 + s, s);
-
-  // prefix of the run: the tile totals before it
-  uint32_t pre = 0;
-  for (int64_t t = tid; t < t0; t += SCAN_THREADS) pre += tile_sum[t];
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) pre += __shfl_xor_sync(0xffffffffu, pre, d);
-  if (lane == 0) s_red[warp] = pre;
-  __syncthreads();
-  uint32_t carry = 0;
-#pragma unroll
-  for (int w = 0; w < SCAN_THREADS / 32; ++w) carry += s_red[w];
-
-  for (int64_t t = t0, it = 0; t < t1; ++t, ++it) {
-    const int s = (int)(it % SSCAN_STAGES);
-    const bool bulk = t < n_full;
-    if (bulk) {
-      const uint32_t parity = (uint32_t)((it / SSCAN_STAGES) & 1);
-      bool ok = false;
-      for (uint32_t spin = 0; spin < SSCAN_SPIN_LIMIT && !(ok = mbar_try_wait(&bar[s], parity)); ++spin) {
-      }
-      if (__syncthreads_or(!ok)) {
-        if (tid == 0) {
-          atomicOr(err, PS_DEVERR_SCAN_TIMEOUT);
-          // let the copies still in flight land before the CTA's shared memory goes
-          for (int64_t u = t; u < t + SSCAN_STAGES && u < t1 && u < n_full; ++u) {
-            const int su = (int)((it + (u - t)) % SSCAN_STAGES);
-            const uint32_t pu = (uint32_t)(((it + (u - t)) / SSCAN_STAGES) & 1);
-            for (uint32_t spin = 0; spin < SSCAN_SPIN_LIMIT && !mbar_try_wait(&bar[su], pu); ++spin) {
-            }
-          }
-        }
-        return;
-      }
-    }
-    // warp w scans elements [w*1024, (w+1)*1024) of the tile; lane l of row k
-    // holds elements 4*(32k + l) .. +3
-    const int64_t wbase = t * SCAN_TILE + (int64_t)warp * (32 * SCAN_ITEMS);
-    uint4 v[ROWS];
-#pragma unroll
-    for (int k = 0; k < ROWS; ++k) {
-      const int64_t e = wbase + 4 * (32 * k + lane);
-      if (bulk) {
-        v[k] = reinterpret_cast<const uint4*>(stage + (size_t)s * SCAN_TILE + warp * (32 * SCAN_ITEMS))[32 * k + lane];
-      } else {
-        v[k].x = e + 0 < n ? in[e + 0] : 0u;
-        v[k].y = e + 1 < n ? in[e + 1] : 0u;
-        v[k].z = e + 2 < n ? in[e + 2] : 0u;
-        v[k].w = e + 3 < n ? in[e + 3] : 0u;
-      }
-    }
-    uint32_t excl[ROWS];
-    uint32_t wsum = 0;
-#pragma unroll
-    for (int k = 0; k < ROWS; ++k) {
-      const uint32_t sum = v[k].x + v[k].y + v[k].z + v[k].w;
-      uint32_t inc = sum;
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t x = __shfl_up_sync(0xffffffffu, inc, d);
-        if (lane >= d) inc += x;
-      }
-      excl[k] = wsum + inc - sum;
-      wsum += __shfl_sync(0xffffffffu, inc, 31);
-    }
-    if (lane == 0) s_warp[warp] = wsum;
-    __syncthreads();  // every warp's total is in, and every thread is done reading stage s
-    if (tid == 0 && bulk) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(t + SSCAN_STAGES, s);
-    }
-    uint32_t off = carry, tile_total = 0;
-#pragma unroll
-    for (int w = 0; w < SCAN_THREADS / 32; ++w) {
-      off += (w < warp) ? s_warp[w] : 0u;
-      tile_total += s_warp[w];
-    }
-#pragma unroll
-    for (int k = 0; k < ROWS; ++k) {
-      const int64_t e = wbase + 4 * (32 * k + lane);
-      uint4 y;
-      y.x = off + excl[k];
-      y.y = y.x + v[k].x;
-      y.z = y.y + v[k].y;
-      y.w = y.z + v[k].z;
-      if (bulk) {
-        *reinterpret_cast<uint4*>(out + e) = y;
-      } else {
-        if (e + 0 < n) out[e + 0] = y.x;
-        if (e + 1 < n) out[e + 1] = y.y;
-        if (e + 2 < n) out[e + 2] = y.z;
-        if (e + 3 < n) out[e + 3] = y.w;
-      }
-    }
-    carry += tile_total;
-    __syncthreads();  // s_warp is reused by the next tile
-  }
-}
-
 }  // namespace psb
