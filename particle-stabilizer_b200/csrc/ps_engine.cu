@@ -469,6 +469,7 @@ void enqueue_regrid(ps_sim* s) {
   const unsigned gp = blocks_for(s->n_total);
   cudaStream_t st = s->stream;
   k_begin<T, MULTI, false, false><<<gb, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
+  k_tile_sums<<<(unsigned)scan_num_tiles(n_scan(s)), STEP_THREADS, 0, st>>>(s->count, n_scan(s), s->tile_sum);
   k_scan_with_tile_sums<<<(unsigned)scan_num_tiles(n_scan(s)), SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s),
                                                                                      s->tile_sum);
   k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,

@@ -124,9 +124,15 @@ __device__ __forceinline__ void walls(vec4_t<T>& P, vec4_t<T>& V, const ScenePar
 // inside the cell is taken later by k_scatter.  The same pass accumulates,
 // warp-aggregated, the per-tile totals of the count array (SCAN_TILE cells
 // per tile) that the step's scan uses in place of a look-back.
+// With tile_sum null only the cell counts are taken (k_tile_sums forms the
+// totals afterwards).
 __device__ __forceinline__ void count_cell(uint32_t* count, uint32_t* tile_sum, uint32_t c, bool valid) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned active = __ballot_sync(0xffffffffu, valid);
+  if (valid && tile_sum == nullptr) {
+    atomicAdd(count + c, 1u);
+    return;
+  }
   if (valid) {
     atomicAdd(count + c, 1u);
     const uint32_t t = c / (uint32_t)SCAN_TILE;
@@ -212,7 +218,28 @@ __global__ void __launch_bounds__(STEP_THREADS) k_begin(StepBufs<T> b, ScenePara
     b.V1[p] = V;
     b.cell[p] = c;
   }
-  count_cell(b.count, b.tile_sum, c, valid);
+  // A regrid (INTEGRATE false) hashes a state in any order, often the
+  // upload's: per-tile totals would take one contended atomic per sphere, so
+  // it counts cells only and k_tile_sums forms the totals.
+  count_cell(b.count, INTEGRATE ? b.tile_sum : nullptr, c, valid);
+}
+
+// tile_sum[t] = sum of count over tile t (SCAN_TILE cells), one CTA per tile.
+__global__ void __launch_bounds__(STEP_THREADS) k_tile_sums(const uint32_t* __restrict__ count, int64_t n,
+                                                           uint32_t* __restrict__ tile_sum) {
+  __shared__ uint32_t s_red[STEP_THREADS / 32];
+  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+  uint32_t sum = 0;
+  for (int64_t e = base + threadIdx.x; e < base + SCAN_TILE && e < n; e += STEP_THREADS) sum += count[e];
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, d);
+  if ((threadIdx.x & 31u) == 0) s_red[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < STEP_THREADS / 32; ++w) t += s_red[w];
+    tile_sum[blockIdx.x] = t;
+  }
 }
 
 constexpr int MOVE_PER_THREAD = 4;
