@@ -11,8 +11,6 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
-#include <condition_variable>
-#include <functional>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -20,7 +18,6 @@
 #include <map>
 #include <mutex>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "particle_stabilizer_b200.h"
@@ -119,10 +116,6 @@ struct ps_sim {
 
   std::map<int64_t, cudaGraphExec_t> graphs;
   int64_t graph_block = 200;  // steps per captured CUDA graph (ps_autotune may change it)
-  // FP32 host transfers: a pinned buffer of 32 B per particle (positions then
-  // velocities as float4) and one event per chunk of a download
-  float4* h_pin = nullptr;
-  std::vector<cudaEvent_t> xfer_events;
   int32_t walk = WALK_LANE;   // neighbour walk of the contact kernel (WALK_LANE / WALK_WARP)
   int32_t contact_block = 256;  // threads per CTA of the contact kernel (WALK_LANE: 128, 256, 512; WALK_WARP: 256)
   int64_t last_launches = 0;
@@ -994,10 +987,6 @@ void free_sim(ps_sim* s) {
   }
   for (auto& kv : s->checkpoints) cudaFree(kv.second);
   s->checkpoints.clear();
-  if (s->h_pin != nullptr) cudaFreeHost(s->h_pin);
-  s->h_pin = nullptr;
-  for (cudaEvent_t e : s->xfer_events) cudaEventDestroy(e);
-  s->xfer_events.clear();
   for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
   s->graphs.clear();
   cudaFree(s->part_arena);
@@ -1297,235 +1286,6 @@ extern "C" int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t 
   return PS_OK;
 }
 
-namespace {
-
-// ---- FP32 host transfers ------------------------------------------------------
-// An FP32 simulation needs 32 B per particle on the device, and the host
-// record is 64 B (8 doubles).  Converting on the host halves the bytes over
-// PCIe, which bound an upload or download: host threads convert one chunk
-// while the copy engine moves the previous one.  double -> float on the host
-// is IEEE round-to-nearest-even, as the device conversion it replaces, and
-// float -> double is exact, so the states are bit-identical.
-
-// Fork-join pool of host threads, shared by all simulations (the caller of
-// run() is one of the workers).
-class HostPool {
- public:
-  static HostPool& get() {
-    static HostPool pool;
-    return pool;
-  }
-  int size() const { return (int)workers_.size() + 1; }
-  // f(k) for k = 0 .. parts-1, spread over the pool; returns when all are done.
-  void run(int parts, const std::function<void(int)>& f) {
-    if (parts <= 0) return;
-    std::lock_guard<std::mutex> one_job(run_mu_);  // one job at a time
-    std::unique_lock<std::mutex> lk(mu_);
-    done_.wait(lk, [&] { return busy_ == 0; });   // no worker is still inside the last job
-    job_ = &f;
-    parts_ = parts;
-    next_.store(0);
-    left_ = parts;
-    ++generation_;
-    cv_.notify_all();
-    lk.unlock();
-    work();
-    lk.lock();
-    done_.wait(lk, [&] { return left_ == 0; });
-    job_ = nullptr;
-  }
-
- private:
-  HostPool() {
-    const unsigned hc = std::thread::hardware_concurrency();
-    const int n = (int)std::max(1u, std::min(hc == 0 ? 1u : hc, 16u)) - 1;
-    for (int t = 0; t < n; ++t) workers_.emplace_back([this] { loop(); });
-  }
-  ~HostPool() {
-    {
-      std::lock_guard<std::mutex> lk(mu_);
-      stop_ = true;
-    }
-    cv_.notify_all();
-    for (auto& t : workers_) t.join();
-  }
-  void loop() {
-    uint64_t seen = 0;
-    for (;;) {
-      std::unique_lock<std::mutex> lk(mu_);
-      cv_.wait(lk, [&] { return stop_ || generation_ != seen; });
-      if (stop_) return;
-      seen = generation_;
-      ++busy_;
-      lk.unlock();
-      work();
-      lk.lock();
-      if (--busy_ == 0) done_.notify_all();
-    }
-  }
-  void work() {
-    for (;;) {
-      const int k = next_.fetch_add(1);
-      if (k >= parts_) return;
-      (*job_)(k);
-      std::lock_guard<std::mutex> lk(mu_);
-      if (--left_ == 0) done_.notify_all();
-    }
-  }
-  std::vector<std::thread> workers_;
-  std::mutex run_mu_, mu_;
-  std::condition_variable cv_, done_;
-  const std::function<void(int)>* job_ = nullptr;
-  std::atomic<int> next_{0};
-  int parts_ = 0, left_ = 0, busy_ = 0;
-  uint64_t generation_ = 0;
-  bool stop_ = false;
-};
-
-constexpr int64_t XFER_CHUNKS = 8;          // copies in flight per transfer
-constexpr int64_t XFER_MIN_PARALLEL = 65536;  // below this many particles one host thread converts
-
-int64_t xfer_chunks(int64_t n) { return n >= XFER_MIN_PARALLEL ? XFER_CHUNKS : 1; }
-
-int ensure_pinned(ps_sim* s) {
-  if (s->h_pin == nullptr) {
-    void* p = nullptr;
-    const cudaError_t e = cudaHostAlloc(&p, 2 * sizeof(float4) * (size_t)std::max<int64_t>(s->n_total, 1),
-                                        cudaHostAllocDefault);
-    if (e != cudaSuccess) return fail(PS_ERR_NOMEM, std::string("pinned host buffer: ") + cudaGetErrorString(e));
-    s->h_pin = static_cast<float4*>(p);
-  }
-  while ((int64_t)s->xfer_events.size() < XFER_CHUNKS) {
-    cudaEvent_t e;
-    PS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    s->xfer_events.push_back(e);
-  }
-  return PS_OK;
-}
-
-// Runs f(a, b) over [k0, k1) split among the pool's threads.
-void host_parallel(int64_t k0, int64_t k1, const std::function<void(int64_t, int64_t)>& f) {
-  const int64_t n = k1 - k0;
-  if (n < XFER_MIN_PARALLEL / XFER_CHUNKS) {
-    f(k0, k1);
-    return;
-  }
-  HostPool& pool = HostPool::get();
-  const int parts = pool.size();
-  const std::function<void(int)> job = [&](int k) {
-    const int64_t a = k0 + n * k / parts, b = k0 + n * (k + 1) / parts;
-    if (a < b) f(a, b);
-  };
-  pool.run(parts, job);
-}
-
-__global__ void k_place_f32(const float4* __restrict__ sP, const float4* __restrict__ sV, float4* P0, float4* V1,
-                            uint32_t* orig, uint32_t n) {
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  P0[p] = sP[p];
-  V1[p] = sV[p];
-  orig[p] = p;
-}
-
-__global__ void k_gather_f32(float4* __restrict__ dP, float4* __restrict__ dV, const float4* P0, const float4* V1,
-                             const uint32_t* orig, uint32_t n) {
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  const uint32_t o = orig[p];
-  dP[o] = P0[p];
-  dV[o] = V1[p];
-}
-
-// FP32 upload: convert (and, for a later upload, check) chunk by chunk into
-// the pinned buffer, copy each chunk into the device staging area as soon as
-// it is converted; only when every record passed the check does the state
-// change.
-int upload_f32(ps_sim* s, const double* aos, int64_t n, bool check) {
-  int rc = ensure_pinned(s);
-  if (rc != PS_OK) return rc;
-  float4* hP = s->h_pin;
-  float4* hV = s->h_pin + n;
-  float4* dP = reinterpret_cast<float4*>(s->staging);
-  float4* dV = dP + n;
-  std::atomic<int64_t> bad{INT64_MAX};
-  const int64_t chunks = xfer_chunks(n);
-  for (int64_t c = 0; c < chunks; ++c) {
-    const int64_t k0 = n * c / chunks, k1 = n * (c + 1) / chunks;
-    host_parallel(k0, k1, [&](int64_t a, int64_t b) {
-      int sc = 0;
-      if (check)
-        while (sc + 1 < s->n_scenes && s->pbase[sc + 1] <= a) ++sc;
-      int64_t first_bad = INT64_MAX;
-      for (int64_t p = a; p < b; ++p) {
-        const double* q = aos + 8 * p;
-        hP[p] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[6]);
-        hV[p] = make_float4((float)q[3], (float)q[4], (float)q[5], (float)q[7]);
-        if (check) {
-          while (sc + 1 < s->n_scenes && s->pbase[sc + 1] <= p) ++sc;
-          if (first_bad == INT64_MAX && (!(2.0 * q[6] <= s->grids[sc].interval) || !(q[7] > 0.0))) first_bad = p;
-        }
-      }
-      int64_t cur = bad.load();
-      while (first_bad < cur && !bad.compare_exchange_weak(cur, first_bad)) {
-      }
-    });
-    PS_CUDA(cudaMemcpyAsync(dP + k0, hP + k0, sizeof(float4) * (size_t)(k1 - k0), cudaMemcpyHostToDevice, s->stream));
-    PS_CUDA(cudaMemcpyAsync(dV + k0, hV + k0, sizeof(float4) * (size_t)(k1 - k0), cudaMemcpyHostToDevice, s->stream));
-  }
-  if (bad.load() != INT64_MAX) {
-    PS_CUDA(cudaStreamSynchronize(s->stream));  // the pinned buffer is free again
-    return fail(PS_ERR_INVALID, "ps_set_state: particle " + std::to_string(bad.load()) +
-                                    " does not fit the grid sized by the first upload");
-  }
-  k_place_f32<<<blocks_for(n), STEP_THREADS, 0, s->stream>>>(dP, dV, static_cast<float4*>(s->P0),
-                                                              static_cast<float4*>(s->V1), s->orig, (uint32_t)n);
-  PS_CUDA(cudaGetLastError());
-  return PS_OK;
-}
-
-// FP32 download: gather into original order on the device, copy chunk by
-// chunk, widen each chunk to the 8-double records as soon as it has landed.
-int download_f32(ps_sim* s, double* out, int64_t n) {
-  int rc = ensure_pinned(s);
-  if (rc != PS_OK) return rc;
-  float4* hP = s->h_pin;
-  float4* hV = s->h_pin + n;
-  float4* dP = reinterpret_cast<float4*>(s->staging);
-  float4* dV = dP + n;
-  k_gather_f32<<<blocks_for(n), STEP_THREADS, 0, s->stream>>>(dP, dV, static_cast<const float4*>(s->P0),
-                                                               static_cast<const float4*>(s->V1), s->orig, (uint32_t)n);
-  PS_CUDA(cudaGetLastError());
-  const int64_t chunks = xfer_chunks(n);
-  for (int64_t c = 0; c < chunks; ++c) {
-    const int64_t k0 = n * c / chunks, k1 = n * (c + 1) / chunks;
-    PS_CUDA(cudaMemcpyAsync(hP + k0, dP + k0, sizeof(float4) * (size_t)(k1 - k0), cudaMemcpyDeviceToHost, s->stream));
-    PS_CUDA(cudaMemcpyAsync(hV + k0, dV + k0, sizeof(float4) * (size_t)(k1 - k0), cudaMemcpyDeviceToHost, s->stream));
-    PS_CUDA(cudaEventRecord(s->xfer_events[(size_t)c], s->stream));
-  }
-  for (int64_t c = 0; c < chunks; ++c) {
-    const int64_t k0 = n * c / chunks, k1 = n * (c + 1) / chunks;
-    PS_CUDA(cudaEventSynchronize(s->xfer_events[(size_t)c]));
-    host_parallel(k0, k1, [&](int64_t a, int64_t b) {
-      for (int64_t p = a; p < b; ++p) {
-        const float4 P = hP[p], V = hV[p];
-        double* q = out + 8 * p;
-        q[0] = P.x;
-        q[1] = P.y;
-        q[2] = P.z;
-        q[3] = V.x;
-        q[4] = V.y;
-        q[5] = V.z;
-        q[6] = P.w;
-        q[7] = V.w;
-      }
-    });
-  }
-  return PS_OK;
-}
-
-}  // namespace
-
 extern "C" int ps_set_state(ps_sim* s, const double* aos, int64_t n_total) {
   if (s == nullptr || (aos == nullptr && n_total > 0)) return fail(PS_ERR_INVALID, "ps_set_state: null argument");
   if (n_total != s->n_total)
@@ -1537,14 +1297,6 @@ extern "C" int ps_set_state(ps_sim* s, const double* aos, int64_t n_total) {
     if (rc != PS_OK) return rc;
   }
   if (n_total == 0) return PS_OK;
-  if (s->precision == PS_FP32) {
-    int rc = upload_f32(s, aos, n_total, !first);
-    if (rc != PS_OK) return rc;
-    rc = regrid(s);  // the state at rest stays in grid order (see below)
-    if (rc != PS_OK) return rc;
-    PS_CUDA(cudaStreamSynchronize(s->stream));
-    return PS_OK;
-  }
   PS_CUDA(cudaMemcpyAsync(s->staging, aos, 64 * (size_t)n_total, cudaMemcpyHostToDevice, s->stream));
   const unsigned g = blocks_for(n_total);
   if (!first) {
@@ -1586,14 +1338,13 @@ extern "C" int ps_get_state(ps_sim* s, double* out, int64_t n_total) {
   if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_get_state: no state uploaded");
   if (n_total == 0) return PS_OK;
   DeviceGuard guard(s->device);
-  if (s->precision == PS_FP32) {
-    const int rc = download_f32(s, out, n_total);
-    if (rc != PS_OK) return rc;
-    return check_device_error(s);
-  }
   const unsigned g = blocks_for(n_total);
-  k_download<double><<<g, STEP_THREADS, 0, s->stream>>>(s->staging, static_cast<vec4_t<double>*>(s->P0),
-                                                        static_cast<vec4_t<double>*>(s->V1), s->orig, (uint32_t)n_total);
+  if (s->precision == PS_FP32)
+    k_download<float><<<g, STEP_THREADS, 0, s->stream>>>(s->staging, static_cast<float4*>(s->P0),
+                                                         static_cast<float4*>(s->V1), s->orig, (uint32_t)n_total);
+  else
+    k_download<double><<<g, STEP_THREADS, 0, s->stream>>>(s->staging, static_cast<vec4_t<double>*>(s->P0),
+                                                          static_cast<vec4_t<double>*>(s->V1), s->orig, (uint32_t)n_total);
   PS_CUDA(cudaGetLastError());
   PS_CUDA(cudaMemcpyAsync(out, s->staging, 64 * (size_t)n_total, cudaMemcpyDeviceToHost, s->stream));
   PS_CUDA(cudaStreamSynchronize(s->stream));
