@@ -180,13 +180,15 @@ def test_bad_inputs_are_errors(need_gpu):
         psb200.Simulation(sc.copy(interval=1e-4), "f32").set_state()  # cell smaller than 2 r_max
 
 
-def test_later_uploads_are_checked_on_the_device(need_gpu):
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_later_uploads_are_checked_on_the_device(need_gpu, precision):
     # after the first upload sizes the grids, a new state is checked on the
     # device: every particle must fit its scene's cell (2 r <= edge) and have
     # a positive mass; the lowest failing index is reported and the previous
     # state stays in place
     batch = [scenes.pile(300, seed=2), scenes.pile(500, seed=3)]
-    with psb200.Simulation(batch, "f64") as sim:
+    rounded = (lambda a: a.astype(np.float32).astype(np.float64)) if precision == "f32" else (lambda a: a)
+    with psb200.Simulation(batch, precision) as sim:
         sim.set_state()
         sim.step(5)
         before = sim.get_state()
@@ -201,4 +203,4 @@ def test_later_uploads_are_checked_on_the_device(need_gpu):
         ok = before.copy()
         ok[420, 6] = 0.5 * edge  # exactly fits
         sim.set_state(ok)
-        assert np.array_equal(sim.get_state(), ok)
+        assert np.array_equal(sim.get_state(), rounded(ok))
