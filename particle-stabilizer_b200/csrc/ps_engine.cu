@@ -7,6 +7,7 @@
 // PhysicsEngineCUDA::startSimulationLoop (PhysicsEngineCUDA.cpp:33-76), which
 // synchronises the device after every one of its 7+ launches per step.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -46,6 +47,18 @@ static int fail(int code, const std::string& msg) {
   } while (0)
 
 extern "C" const char* ps_last_error(void) { return g_last_error.c_str(); }
+
+namespace {
+// NVTX range around an entry point, so a profiler's timeline shows the
+// library's calls (no cost without an attached tool: NVTX is header-only and
+// loads its back end only when one is present).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+}  // namespace
 
 extern "C" int ps_internal_fail(int code, const char* msg) { return fail(code, msg ? msg : ""); }
 
@@ -1287,6 +1300,7 @@ extern "C" int ps_create(const ps_scene_desc* scenes, int32_t n_scenes, int32_t 
 }
 
 extern "C" int ps_set_state(ps_sim* s, const double* aos, int64_t n_total) {
+  const NvtxRange nvtx_range("ps_set_state");
   if (s == nullptr || (aos == nullptr && n_total > 0)) return fail(PS_ERR_INVALID, "ps_set_state: null argument");
   if (n_total != s->n_total)
     return fail(PS_ERR_INVALID, "ps_set_state: expected " + std::to_string(s->n_total) + " particles, got " + std::to_string(n_total));
@@ -1333,6 +1347,7 @@ extern "C" int ps_set_state(ps_sim* s, const double* aos, int64_t n_total) {
 }
 
 extern "C" int ps_get_state(ps_sim* s, double* out, int64_t n_total) {
+  const NvtxRange nvtx_range("ps_get_state");
   if (s == nullptr || (out == nullptr && n_total > 0)) return fail(PS_ERR_INVALID, "ps_get_state: null argument");
   if (n_total != s->n_total) return fail(PS_ERR_INVALID, "ps_get_state: size mismatch");
   if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_get_state: no state uploaded");
@@ -1511,6 +1526,7 @@ extern "C" int ps_list_stats(ps_sim* s, int64_t* rebuilds, int64_t* fallbacks, i
 }
 
 extern "C" int ps_step(ps_sim* s, int64_t n_steps) {
+  const NvtxRange nvtx_range("ps_step");
   if (s == nullptr || n_steps < 0) return fail(PS_ERR_INVALID, "ps_step: bad argument");
   if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_step: call ps_set_state first");
   s->last_launches = 0;
@@ -1612,6 +1628,7 @@ int resize_grids(ps_sim* s, const std::vector<double>& host_state) {
 
 extern "C" int ps_autotune(ps_sim* s, int64_t trial_steps, const double* cell_factors, int32_t n_factors,
                            const int64_t* graph_blocks, int32_t n_blocks, double* ms_table, ps_tune_result* out) {
+  const NvtxRange nvtx_range("ps_autotune");
   if (s == nullptr || out == nullptr || trial_steps < 1 || cell_factors == nullptr || n_factors < 1 ||
       graph_blocks == nullptr || n_blocks < 1)
     return fail(PS_ERR_INVALID, "ps_autotune: bad argument");
@@ -1742,6 +1759,7 @@ extern "C" int ps_get_contact_kernel(ps_sim* s, int32_t* walk, int32_t* block) {
 
 extern "C" int ps_tune_neighbor_lists(ps_sim* s, int64_t trial_steps, const double* skins, int32_t n_skins,
                                       int32_t max_neighbours, double* ms_table, double* best_skin) {
+  const NvtxRange nvtx_range("ps_tune_neighbor_lists");
   if (s == nullptr || best_skin == nullptr || trial_steps < 1 || skins == nullptr || n_skins < 1 ||
       max_neighbours < 1 || max_neighbours > 4096)
     return fail(PS_ERR_INVALID, "ps_tune_neighbor_lists: bad argument");
@@ -1830,6 +1848,7 @@ extern "C" int ps_profile_steps(ps_sim* s, int64_t n_steps, double* kernel_ms, i
 }
 
 extern "C" int ps_forward_checkpointed(ps_sim* s, int64_t n_steps, int64_t every) {
+  const NvtxRange nvtx_range("ps_forward_checkpointed");
   if (s == nullptr || n_steps < 1 || every < 1) return fail(PS_ERR_INVALID, "ps_forward_checkpointed: bad argument");
   if (!s->grid_sized) return fail(PS_ERR_INVALID, "ps_forward_checkpointed: call ps_set_state first");
   if (s->has_mesh) return fail(PS_ERR_INVALID, "ps_forward_checkpointed: differentiation supports box containers only");
@@ -1850,6 +1869,7 @@ extern "C" int ps_forward_checkpointed(ps_sim* s, int64_t n_steps, int64_t every
 }
 
 extern "C" int ps_backward(ps_sim* s, const double* dl_dstate, ps_grad* grads, double* dl_dstate0) {
+  const NvtxRange nvtx_range("ps_backward");
   if (s == nullptr || dl_dstate == nullptr || grads == nullptr) return fail(PS_ERR_INVALID, "ps_backward: null argument");
   if (s->fwd_steps < 1) return fail(PS_ERR_INVALID, "ps_backward: call ps_forward_checkpointed first");
   DeviceGuard guard(s->device);
