@@ -94,6 +94,13 @@ typedef struct ps_sim ps_sim;
 /* Message of this thread's last failure ("" if none). */
 const char* ps_last_error(void);
 
+/* 1 when this library is the bounds-checked build (compiled with
+ * -DPS_DEBUG_BOUNDS, lib_debug/): device indexes into the bucket, order and
+ * state arrays are checked, an index out of range is skipped and the call
+ * that syncs next fails with PS_ERR_DEVICE; 0 for the product build.  No
+ * counterpart in the reference. */
+int32_t ps_bounds_checked(void);
+
 /* Create a simulation of n_scenes independent scenes on CUDA device
  * `device`, in PS_FP32 or PS_FP64.  One scene replaces the set-up half of
  * runSimulateCUDA: ParticleModelCUDA ctor + container ctor + initBuckets

@@ -170,6 +170,25 @@ enum : uint32_t {
   PS_DEVERR_BAD_CELL = 1u << 2,       // a cell id fell outside its scene (never expected)
   PS_DEVERR_LIST_OVERFLOW = 1u << 3,  // neighbour-list mode: a list or a sphere's overlap buffer was full
   PS_DEVERR_LIST_BARRIER = 1u << 4,   // neighbour-list mode: a grid barrier of the rebuild gave up waiting
+  PS_DEVERR_BOUNDS = 1u << 5,         // bounds-checked build: an index fell outside its array
 };
+
+// Bounds-checked build (compiled with -DPS_DEBUG_BOUNDS, `make debug`):
+// in_bounds(i, n, err) is false when i >= n, records PS_DEVERR_BOUNDS, and
+// the caller skips the access, so a wrong index shows up as an error status
+// instead of a memory fault.  In the product build it is the constant true
+// and costs nothing.
+__device__ __forceinline__ bool in_bounds(uint64_t i, uint64_t n, uint32_t* err) {
+#ifdef PS_DEBUG_BOUNDS
+  if (i < n) return true;
+  atomicOr(err, PS_DEVERR_BOUNDS);
+  return false;
+#else
+  (void)i;
+  (void)n;
+  (void)err;
+  return true;
+#endif
+}
 
 }  // namespace psb

@@ -48,6 +48,14 @@ static int fail(int code, const std::string& msg) {
 
 extern "C" const char* ps_last_error(void) { return g_last_error.c_str(); }
 
+extern "C" int32_t ps_bounds_checked(void) {
+#ifdef PS_DEBUG_BOUNDS
+  return 1;
+#else
+  return 0;
+#endif
+}
+
 namespace {
 // NVTX range around an entry point, so a profiler's timeline shows the
 // library's calls (no cost without an attached tool: NVTX is header-only and
@@ -203,6 +211,7 @@ StepBufs<T> bufs(ps_sim* s) {
   b.scell = s->scell;
   b.bounds = static_cast<const T*>(s->d_bounds);
   b.n_tiles = (uint32_t)scan_num_tiles(n_scan(s));
+  b.n_scan = (uint32_t)n_scan(s);
   b.tape_p = nullptr;
   b.tape_v = nullptr;
   b.tape_vpre = nullptr;
@@ -282,7 +291,7 @@ int64_t enqueue_steps(ps_sim* s, int64_t steps) {
     pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, nsc,
                (const uint32_t*)s->tile_sum);
     pdl_launch(k_scatter, move_blocks(s->n_total, b.n_tiles), STEP_THREADS, st, (const uint32_t*)s->cell, s->slot,
-               (const uint32_t*)s->orig, (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles);
+               (const uint32_t*)s->orig, (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles, s->err);
     pdl_launch(k_rank_move<T>, move_blocks(s->n_total, 0), STEP_THREADS, st, b);
     if (k + 1 < steps) {
       const auto c = contacts_kernel<T, MULTI, MESH, true>(s);
@@ -325,7 +334,7 @@ void enqueue_steps_recorded(ps_sim* s, int64_t steps, std::vector<LaunchRecord>&
     post();
     pre(PS_K_SCATTER);
     k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
-                                                                         s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
+                                                                         s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles, s->err);
     post();
     pre(PS_K_RANK_MOVE);
     k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
@@ -407,7 +416,7 @@ cudaError_t enqueue_steps_list(ps_sim* s, int64_t steps) {
   pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, nsc,
              (const uint32_t*)s->tile_sum);
   pdl_launch(k_scatter, gm0, STEP_THREADS, st, (const uint32_t*)s->cell, s->slot, (const uint32_t*)s->orig,
-             (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles);
+             (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles, s->err);
   pdl_launch(k_rank_move<T>, gm1, STEP_THREADS, st, b);
   pdl_launch(k_list_build<T, MULTI>, gp, STEP_THREADS, st, b, sp0, L, 0);
   for (int64_t k = 0; k < steps; ++k) {
@@ -486,7 +495,7 @@ void enqueue_regrid(ps_sim* s) {
   k_scan_with_tile_sums<<<(unsigned)scan_num_tiles(n_scan(s)), SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s),
                                                                                      s->tile_sum);
   k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
-                                                                       s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles);
+                                                                       s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles, s->err);
   k_rank_move<T><<<move_blocks(s->n_total, 0), STEP_THREADS, 0, st>>>(b);
   k_copy_vel<T><<<gp, STEP_THREADS, 0, st>>>(b);
 }
@@ -514,6 +523,7 @@ int check_device_error(ps_sim* s) {
     if (e & PS_DEVERR_SCAN_TIMEOUT) m += " scan look-back wait expired;";
     if (e & PS_DEVERR_MESH_OVERFLOW) m += " a particle hit more than 64 triangles in one step;";
     if (e & PS_DEVERR_BAD_CELL) m += " cell id outside its scene;";
+    if (e & PS_DEVERR_BOUNDS) m += " index out of bounds (bounds-checked build; the access was skipped);";
     uint32_t zero = 0;
     cudaMemcpyAsync(s->err, &zero, sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream);
     cudaStreamSynchronize(s->stream);
@@ -777,7 +787,14 @@ int upload_mesh(ps_sim* s) {
   PS_CUDA(cudaMemcpy(s->d_bin_offset, bin_offset.data(), bin_offset.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
   if (!bin_tri.empty())
     PS_CUDA(cudaMemcpy(s->d_bin_tri, bin_tri.data(), bin_tri.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-  const MeshView mv{s->d_tri, s->d_nrm, s->d_aabb, s->d_bin_offset, s->d_bin_tri};
+  const MeshView mv{s->d_tri,
+                    s->d_nrm,
+                    s->d_aabb,
+                    s->d_bin_offset,
+                    s->d_bin_tri,
+                    (uint32_t)s->tri_total,
+                    (uint32_t)s->bins_total,
+                    (uint32_t)bin_tri.size()};
   PS_CUDA(cudaMemcpy(s->d_mesh_view, &mv, sizeof(MeshView), cudaMemcpyHostToDevice));
   return PS_OK;
 }
@@ -1105,7 +1122,7 @@ int enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes, 
                (const uint32_t*)s->tile_sum);
     pdl_launch(k_scatter, move_blocks(s->n_total, b.n_tiles), STEP_THREADS, st, (const uint32_t*)s->cell, s->slot,
                (const uint32_t*)s->orig, (const uint32_t*)off_k, s->tmp, s->count, (uint32_t)s->n_total,
-               s->tile_sum, b.n_tiles);
+               s->tile_sum, b.n_tiles, s->err);
     pdl_launch(k_rank_move<T>, move_blocks(s->n_total, 0), STEP_THREADS, st, b);
     b.tape_vpre = row.vpre;
     b.tape_cell = row.cell;

@@ -106,6 +106,7 @@ __device__ __forceinline__ void list_build_one(uint32_t i, const StepBufs<T>& b,
     const uint32_t ny = (uint32_t)sp.nb[1], nz = (uint32_t)sp.nb[2];
     // candidates of one column's slot range [j0, j1)
     auto walk = [&](uint32_t j0, uint32_t j1) {
+      if (!in_bounds(j1, (uint64_t)b.n + 1u, b.err)) return;
       for (uint32_t j = j0; j < j1; ++j) {
         if (j == i) continue;
         const vec4_t<T> Q = ld4c<T, COH>(b.P0 + j);
@@ -216,7 +217,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_list_rebuild(StepBufs<T> b, Sc
   }
   if (!grid_barrier(bar, b.err)) return;
   for (uint32_t blk = blockIdx.x; blk < scatter_blocks; blk += gridDim.x)
-    scatter_block<true>(blk, b.cell, b.slot, b.orig, b.offset, b.tmp, b.count, b.n, b.tile_sum, b.n_tiles);
+    scatter_block<true>(blk, b.cell, b.slot, b.orig, b.offset, b.tmp, b.count, b.n, b.tile_sum, b.n_tiles, b.err);
   if (!grid_barrier(bar, b.err)) return;
   for (uint32_t blk = blockIdx.x; blk < move_blocks; blk += gridDim.x) rank_move_block<T, true>(blk, b);
   if (!grid_barrier(bar, b.err)) return;
@@ -295,7 +296,10 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 4 : 3)
         uint32_t jj[NB];
         vec4_t<T> QQ[NB];
 #pragma unroll
-        for (int u = 0; u < NB; ++u) jj[u] = k0 + u < nl ? L.list[(size_t)(k0 + u) * b.n + i] : i;
+        for (int u = 0; u < NB; ++u) {
+          jj[u] = k0 + u < nl ? L.list[(size_t)(k0 + u) * b.n + i] : i;
+          if (!in_bounds(jj[u], b.n, b.err)) jj[u] = i;
+        }
 #pragma unroll
         for (int u = 0; u < NB; ++u) QQ[u] = ld4<T>(Ps + jj[u]);
 #pragma unroll
@@ -322,6 +326,7 @@ __global__ void __launch_bounds__(STEP_THREADS, sizeof(T) == 4 ? 4 : 3)
         int nc = 0;
         for (uint32_t k = 0; k < nl; ++k) {
           const uint32_t j = L.list[(size_t)k * b.n + i];
+          if (!in_bounds(j, b.n, b.err)) continue;
           uint64_t kj;
           if (!list_pair<T>(L, b, sp, src, P, ld4<T>(Ps + j), j, cx, cy, cz, kj)) continue;
           if (nc == LIST_CONTACTS_MAX) {

@@ -36,6 +36,9 @@ struct MeshView {
   const void* aabb;
   const uint32_t* bin_offset;
   const uint32_t* bin_tri;
+  uint32_t n_tri;      // triangles over all scenes
+  uint32_t n_bins;     // bins over all scenes (bin_offset holds n_bins + 1)
+  uint32_t n_bin_tri;  // entries of bin_tri
 };
 
 template <class T>
@@ -139,9 +142,12 @@ __device__ void mesh_contacts(vec4_t<T>& P, vec4_t<T>& V, const SceneParams<T>& 
         const uint32_t bin = sp.mesh_bin_base +
                              ((uint32_t)bx * (uint32_t)sp.mesh_nb[1] + (uint32_t)by) * (uint32_t)sp.mesh_nb[2] +
                              (uint32_t)bz;
+        if (!in_bounds(bin, mvv.n_bins, err)) continue;
         const uint32_t t0 = __ldg(mv.bin_offset + bin), t1 = __ldg(mv.bin_offset + bin + 1);
+        if (!in_bounds(t1, (uint64_t)mvv.n_bin_tri + 1u, err)) continue;
         for (uint32_t s = t0; s < t1; ++s) {
           const uint32_t t = __ldg(mv.bin_tri + s);
+          if (!in_bounds(t, mvv.n_tri, err)) continue;
           const T* bb = mv.aabb + 6 * (size_t)t;
           // closed AABB test (isIntersectedKernel :191-197)
           if (!(lox <= bb[3] && hix >= bb[0] && loy <= bb[4] && hiy >= bb[1] && loz <= bb[5] && hiz >= bb[2]))

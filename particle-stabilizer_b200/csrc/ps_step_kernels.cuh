@@ -166,6 +166,7 @@ struct StepBufs {
   uint32_t n;             // particles over all scenes
   uint32_t* tile_sum;     // per-tile totals of `count`, cleared by k_scatter
   uint32_t n_tiles;
+  uint32_t n_scan;        // entries of count and offset (cells over all scenes + 1)
   uint32_t* scell;        // global cell id of each sorted slot (written by k_rank_move)
   const T* bounds;        // per-scene, per-axis cell boundaries (see SceneParams::bnd_base)
   // Optional tape row (null outside the adjoint's recompute): k_contacts
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_begin(StepBufs<T> b, ScenePara
   // A regrid (INTEGRATE false) hashes a state in any order, often the
   // upload's: per-tile totals would take one contended atomic per sphere, so
   // it counts cells only and k_tile_sums forms the totals.
-  count_cell(b.count, INTEGRATE ? b.tile_sum : nullptr, c, valid);
+  count_cell(b.count, INTEGRATE ? b.tile_sum : nullptr, c, valid && in_bounds(c, b.n_scan - 1u, b.err));
 }
 
 // tile_sum[t] = sum of count over tile t (SCAN_TILE cells), one CTA per tile.
@@ -263,7 +264,7 @@ template <bool COH>
 __device__ __forceinline__ void scatter_block(uint32_t blk, const uint32_t* __restrict__ cell,
                                               uint32_t* __restrict__ slot, const uint32_t* __restrict__ orig,
                                               const uint32_t* __restrict__ offset, uint32_t* tmp, uint32_t* count,
-                                              uint32_t n, uint32_t* tile_sum, uint32_t n_tiles) {
+                                              uint32_t n, uint32_t* tile_sum, uint32_t n_tiles, uint32_t* err) {
   const uint32_t t = blk * STEP_THREADS + threadIdx.x;
   if (t < n_tiles) tile_sum[t] = 0u;
   const uint32_t base = blk * (STEP_THREADS * MOVE_PER_THREAD) + threadIdx.x;
@@ -284,7 +285,7 @@ __device__ __forceinline__ void scatter_block(uint32_t blk, const uint32_t* __re
   }
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
-    if (base + k * STEP_THREADS < n) {
+    if (base + k * STEP_THREADS < n && in_bounds(off[k] + sl[k], n, err)) {
       tmp[off[k] + sl[k]] = o[k];
       slot[base + k * STEP_THREADS] = nxt[k] - off[k] == 1u ? (off[k] | SLOT_ALONE) : sl[k];
     }
@@ -296,9 +297,9 @@ __global__ void __launch_bounds__(STEP_THREADS) k_scatter(const uint32_t* __rest
                                                           const uint32_t* __restrict__ orig,
                                                           const uint32_t* __restrict__ offset, uint32_t* tmp,
                                                           uint32_t* count, uint32_t n, uint32_t* tile_sum,
-                                                          uint32_t n_tiles) {
+                                                          uint32_t n_tiles, uint32_t* err) {
   pdl_wait();
-  scatter_block<false>(blockIdx.x, cell, slot, orig, offset, tmp, count, n, tile_sum, n_tiles);
+  scatter_block<false>(blockIdx.x, cell, slot, orig, offset, tmp, count, n, tile_sum, n_tiles, err);
 }
 
 // Canonical position = offset[c] + #{members of c with a smaller orig id};
@@ -335,14 +336,16 @@ __device__ __forceinline__ void rank_move_block(uint32_t blk, const StepBufs<T>&
   }
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k)
-    o[k] = base + k * STEP_THREADS < b.n ? b.tmp[start[k] + sl[k]] : 0u;
+    o[k] = (base + k * STEP_THREADS < b.n && in_bounds(start[k] + sl[k], b.n, b.err)) ? b.tmp[start[k] + sl[k]] : 0u;
 #pragma unroll
   for (int k = 0; k < MOVE_PER_THREAD; ++k) {
     if (base + k * STEP_THREADS >= b.n) continue;
+    if (!in_bounds(end[k], b.n + 1u, b.err)) continue;
     uint32_t rank = 0;
     if (end[k] - start[k] > 1u)
       for (uint32_t s = start[k]; s < end[k]; ++s) rank += (b.tmp[s] < o[k]) ? 1u : 0u;
     const uint32_t d = start[k] + rank;
+    if (!in_bounds(d, b.n, b.err)) continue;
     b.P0[d] = P[k];
     b.V0[d] = V[k];
     b.orig[d] = o[k];
@@ -545,8 +548,10 @@ __global__ void __launch_bounds__(BLOCK, contact_min_blocks<T, BLOCK>()) k_conta
     const bool ok = live && bx >= 0 && bx < nx && by >= 0 && by < ny;
     // in-range address even where the column does not exist
     const uint32_t col = ok ? sp.cbase + ((uint32_t)bx * (uint32_t)ny + (uint32_t)by) * (uint32_t)nz : sp.cbase;
-    lo[q] = ok ? __ldg(b.offset + col + z0) : 0u;
-    hi[q] = ok ? __ldg(b.offset + col + z1) : 0u;
+    const bool inb = ok && in_bounds(col + z1, b.n_scan, b.err);
+    lo[q] = inb ? __ldg(b.offset + col + z0) : 0u;
+    hi[q] = inb ? __ldg(b.offset + col + z1) : 0u;
+    if (!in_bounds(hi[q], b.n + 1u, b.err)) hi[q] = lo[q] = 0u;
   }
   const T ks = sp.k_spring, es = sp.e_sphere;
   if constexpr (WALK == WALK_LANE) {
@@ -609,7 +614,7 @@ __global__ void __launch_bounds__(BLOCK, contact_min_blocks<T, BLOCK>()) k_conta
     }
   }
   if (FUSED) {
-    count_cell(b.count, b.tile_sum, c, valid);
+    count_cell(b.count, b.tile_sum, c, valid && in_bounds(c, b.n_scan - 1u, b.err));
   }
 }
 

@@ -16,6 +16,9 @@ from .scenes import Scene  # noqa: F401
 
 PKG_ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 LIB_PATH = os.path.join(PKG_ROOT, "lib", "libparticle_stabilizer_cuda.so")
+# the bounds-checked build of the same library (`make debug`); point LIB_PATH
+# at it before the first lib() call to run everything through it
+DEBUG_LIB_PATH = os.path.join(PKG_ROOT, "lib_debug", "libparticle_stabilizer_cuda.so")
 CLI_PATH = os.path.join(PKG_ROOT, "bin", "particle_stabilizer_main")
 
 PS_OK = 0
@@ -29,7 +32,7 @@ EXPORTED = (
     "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "ps_forward_checkpointed",
     "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_exclusive_scan_u32_noalloc_status", "ps_autotune", "ps_set_contact_kernel", "ps_get_contact_kernel", "ps_set_neighbor_lists", "ps_list_stats", "ps_tune_neighbor_lists",
     "ps_resolve_overlaps", "ps_overlap_stats",
-    "ps_write_obj_spheres", "runSimulateCUDA",
+    "ps_write_obj_spheres", "ps_bounds_checked", "runSimulateCUDA",
 )
 KERNEL_KINDS = ("begin", "scan", "scatter", "rank_move", "contacts")
 
@@ -86,6 +89,7 @@ def lib() -> C.CDLL:
             raise PSError(f"{LIB_PATH} is missing: build it with `make -C particle-stabilizer_b200`")
         L = C.CDLL(LIB_PATH)
         L.ps_last_error.restype = C.c_char_p
+        L.ps_bounds_checked.restype = C.c_int32
         L.ps_create.argtypes = [C.POINTER(SceneDesc), C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
         L.ps_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
         L.ps_get_state.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
@@ -377,6 +381,13 @@ def exclusive_scan_u32_noalloc_status(stream: int = 0) -> int:
     _check(lib().ps_exclusive_scan_u32_noalloc_status(C.c_void_p(stream), C.byref(w)),
            "ps_exclusive_scan_u32_noalloc_status")
     return int(w.value)
+
+
+def bounds_checked() -> bool:
+    """ps_bounds_checked: True when the loaded library is the bounds-checked
+    build, whose out-of-range device indexes are skipped and reported as
+    PS_ERR_DEVICE instead of faulting."""
+    return bool(lib().ps_bounds_checked())
 
 
 def exclusive_scan_scratch_bytes(n: int) -> int:

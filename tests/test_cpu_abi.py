@@ -111,3 +111,19 @@ def test_cli_help_and_missing_input(tmp_path):
     r = subprocess.run([exe, "--lib", str(tmp_path / "nolib.so"), "x.csv"], capture_output=True, text=True,
                        cwd=tmp_path)
     assert r.returncode != 0 and "Cannot open library" in r.stderr
+
+
+def test_bounds_checked_build_exports_the_same_symbols():
+    """lib_debug/ (make debug) is the same C ABI compiled with
+    -DPS_DEBUG_BOUNDS; ps_bounds_checked tells the two builds apart."""
+    assert os.path.exists(psb200.DEBUG_LIB_PATH), "build it with `make -C particle-stabilizer_b200 debug`"
+    out = subprocess.run(["nm", "-D", "--defined-only", psb200.DEBUG_LIB_PATH], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    assert set(declared_functions()) <= exported and set(psb200.EXPORTED) <= exported
+    assert psb200.bounds_checked() is False
+    code = ("import psb200; psb200.LIB_PATH = psb200.DEBUG_LIB_PATH; "
+            "assert psb200.bounds_checked() is True; print('checked')")
+    env = dict(os.environ)
+    env["PYTHONPATH"] = os.pathsep.join([ROOT, os.path.join(ROOT, "particle-stabilizer_b200", "python")])
+    r = subprocess.run(["python3", "-c", code], capture_output=True, text=True, env=env)
+    assert r.returncode == 0 and "checked" in r.stdout, r.stderr
