@@ -5,11 +5,18 @@
  * -ffp-contract=off so the compiler adds no fused operations of its own:
  * the only fused multiply-adds are the explicit fma()/fmaf() calls.
  */
+#define _DEFAULT_SOURCE /* sysconf */
 #include "ps_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
+
+/* host threads for the triangle pass of large calls */
+#define OR_MAX_THREADS 64
 
 /* ---- grid (ParticleModelCUDA.cpp:62-113, ParticleBucket.cpp:17-27) ---- */
 double or_interval_cuda(double r_max) { return r_max * 2.0 * 1.05; }
