@@ -1,7 +1,7 @@
 /*
  * ps_oracle.h — CPU oracle for the particle-stabilizer DEM step.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker: only tests/,
+ * TEST INFRASTRUCTURE ONLY.  Only tests/,
  * __graft_entry__.smoke() and the cpu_baseline leg of bench.py may load it.
  * The product library (libparticle_stabilizer_cuda.so) never links it.
  *

@@ -1,7 +1,7 @@
 """ctypes binding of the C oracle and of the reference builds under oracle/_ref.
 
 TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and
-bench.py's cpu_baseline / reference legs, as the checker.  The product path
+bench.py's cpu_baseline / reference legs, to check results.  The product path
 never imports this module.
 
 State arrays are (n, 8) in the reference's ParticlePrimitive layout

@@ -4,7 +4,7 @@
 // Same flags, defaults and file formats.  Like the reference's --cuda path it
 // loads ./libparticle_stabilizer_cuda.so with dlopen and calls its
 // runSimulateCUDA symbol (ParticleStabilizerMain.cpp:19-21,235-256).  The
-// reference's CPU simulator is not part of this build: the B200 path runs
+// reference's CPU simulator is not part of this program: the B200 path runs
 // whether or not --cuda is given.  Extra flags: --fp32 (single precision),
 // --cell-size S, --widen-domain, --lib PATH.  --visualize has no graphics
 // stack to open and is reported and skipped.  After the run, as the
@@ -129,7 +129,7 @@ int main(int argc, char** argv) {
     std::cerr << "Cannot load symbol: 'runSimulateCUDA' from the shared library.\n";
     return EXIT_FAILURE;
   }
-  if (!a.toUseCUDA) std::cout << "[info] this build runs the B200 path (--cuda implied)\n";
+  if (!a.toUseCUDA) std::cout << "[info] this program runs the B200 path (--cuda implied)\n";
 
   // ParticleData::readFromCSV (ParticleIO.cpp:90-144)
   const double vel[3] = {a.initialVelocity.x, a.initialVelocity.y, a.initialVelocity.z};
