@@ -166,7 +166,7 @@ inline void fast_udiv_magic(uint32_t d, uint32_t& m, uint32_t& sh1, uint32_t& sh
 // Device error word bits (read by the host after a step block).
 enum : uint32_t {
   PS_DEVERR_SCAN_TIMEOUT = 1u << 0,   // decoupled look-back gave up waiting
-  PS_DEVERR_MESH_OVERFLOW = 1u << 1,  // a particle hit more triangles than the hit buffer holds
+  PS_DEVERR_MESH_OVERFLOW = 1u << 1,  // reserved: hits beyond the buffer now take further passes
   PS_DEVERR_BAD_CELL = 1u << 2,       // a cell id fell outside its scene (never expected)
   PS_DEVERR_LIST_OVERFLOW = 1u << 3,  // neighbour-list mode: a list or a sphere's overlap buffer was full
   PS_DEVERR_LIST_BARRIER = 1u << 4,   // neighbour-list mode: a grid barrier of the rebuild gave up waiting

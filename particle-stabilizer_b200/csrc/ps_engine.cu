@@ -521,7 +521,6 @@ int check_device_error(ps_sim* s) {
   if (e != 0) {
     std::string m = "device error word 0x" + std::to_string(e) + ":";
     if (e & PS_DEVERR_SCAN_TIMEOUT) m += " scan look-back wait expired;";
-    if (e & PS_DEVERR_MESH_OVERFLOW) m += " a particle hit more than 64 triangles in one step;";
     if (e & PS_DEVERR_BAD_CELL) m += " cell id outside its scene;";
     if (e & PS_DEVERR_BOUNDS) m += " index out of bounds (bounds-checked build; the access was skipped);";
     uint32_t zero = 0;

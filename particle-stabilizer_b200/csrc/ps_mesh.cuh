@@ -116,14 +116,16 @@ __device__ __forceinline__ int32_t mesh_axis(T x, T lo, T iv, int32_t nb) {
   return (int32_t)q;
 }
 
+// Hits of one pass: walks the bins the sphere's AABB covers and keeps, in
+// ascending order, the MESH_MAX_HITS smallest ids of the triangles it hits
+// (above `after` unless `first`); true if a hit was left for a later pass.
 template <class T>
-__device__ void mesh_contacts(vec4_t<T>& P, vec4_t<T>& V, const SceneParams<T>& sp, const MeshView& mvv,
-                              uint32_t* err) {
+__device__ __forceinline__ bool mesh_collect(const V3<T>& c, T r, const SceneParams<T>& sp, const MeshView& mvv,
+                                             uint32_t* err, bool first, uint32_t after,
+                                             uint32_t (&hits)[MESH_MAX_HITS], int& nh) {
   using A = Ar<T>;
   const MeshViewT<T> mv{static_cast<const T*>(mvv.tri), static_cast<const T*>(mvv.nrm),
                         static_cast<const T*>(mvv.aabb), mvv.bin_offset, mvv.bin_tri};
-  const T r = P.w;
-  const V3<T> c = {P.x, P.y, P.z};
   const T lox = A::sub(c.x, r), loy = A::sub(c.y, r), loz = A::sub(c.z, r);
   const T hix = A::add(c.x, r), hiy = A::add(c.y, r), hiz = A::add(c.z, r);
   const int32_t bx0 = mesh_axis<T>(lox, sp.mesh_lo[0], sp.mesh_iv, sp.mesh_nb[0]);
@@ -132,10 +134,8 @@ __device__ void mesh_contacts(vec4_t<T>& P, vec4_t<T>& V, const SceneParams<T>& 
   const int32_t bx1 = mesh_axis<T>(hix, sp.mesh_lo[0], sp.mesh_iv, sp.mesh_nb[0]);
   const int32_t by1 = mesh_axis<T>(hiy, sp.mesh_lo[1], sp.mesh_iv, sp.mesh_nb[1]);
   const int32_t bz1 = mesh_axis<T>(hiz, sp.mesh_lo[2], sp.mesh_iv, sp.mesh_nb[2]);
-
-  uint32_t hits[MESH_MAX_HITS];
-  int nh = 0;
-  bool overflow = false;
+  nh = 0;
+  bool more = false;
   for (int32_t bx = bx0; bx <= bx1; ++bx)
     for (int32_t by = by0; by <= by1; ++by)
       for (int32_t bz = bz0; bz <= bz1; ++bz) {
@@ -148,6 +148,7 @@ __device__ void mesh_contacts(vec4_t<T>& P, vec4_t<T>& V, const SceneParams<T>& 
         for (uint32_t s = t0; s < t1; ++s) {
           const uint32_t t = __ldg(mv.bin_tri + s);
           if (!in_bounds(t, mvv.n_tri, err)) continue;
+          if (!first && t <= after) continue;  // applied by an earlier pass
           const T* bb = mv.aabb + 6 * (size_t)t;
           // closed AABB test (isIntersectedKernel :191-197)
           if (!(lox <= bb[3] && hix >= bb[0] && loy <= bb[4] && hiy >= bb[1] && loz <= bb[5] && hiz >= bb[2]))
@@ -160,6 +161,10 @@ __device__ void mesh_contacts(vec4_t<T>& P, vec4_t<T>& V, const SceneParams<T>& 
               mesh_axis<T>(iy, sp.mesh_lo[1], sp.mesh_iv, sp.mesh_nb[1]) != by ||
               mesh_axis<T>(iz, sp.mesh_lo[2], sp.mesh_iv, sp.mesh_nb[2]) != bz)
             continue;
+          if (nh == MESH_MAX_HITS && t > hits[nh - 1]) {  // a later pass takes it
+            more = true;
+            continue;
+          }
           const T* tv = mv.tri + 9 * (size_t)t;
           const T* tn = mv.nrm + 3 * (size_t)t;
           const V3<T> a = {tv[0], tv[1], tv[2]}, b = {tv[3], tv[4], tv[5]}, cc = {tv[6], tv[7], tv[8]};
@@ -167,26 +172,36 @@ __device__ void mesh_contacts(vec4_t<T>& P, vec4_t<T>& V, const SceneParams<T>& 
           const V3<T> cp = tri_closest<T>(a, b, cc, n, c, sp.edge_quirk);
           const V3<T> rel = v3sub(cp, c);
           if (!(v3dot(rel, rel) < A::mul(r, r))) continue;
-          // insert keeping ascending triangle order
-          if (nh < MESH_MAX_HITS) {
-            int k = nh++;
-            while (k > 0 && hits[k - 1] > t) {
-              hits[k] = hits[k - 1];
-              --k;
-            }
-            hits[k] = t;
-          } else {
-            overflow = true;
+          if (nh == MESH_MAX_HITS) {  // full: the largest kept id moves to a later pass
+            more = true;
+            --nh;
           }
+          // insert keeping ascending triangle order
+          int k = nh++;
+          while (k > 0 && hits[k - 1] > t) {
+            hits[k] = hits[k - 1];
+            --k;
+          }
+          hits[k] = t;
         }
       }
-  if (overflow) atomicOr(err, PS_DEVERR_MESH_OVERFLOW);
-  T svx = 0, svy = 0, svz = 0, mx = 0, my = 0, mz = 0;
-  const T e = sp.e_poly;
+  return more;
+}
+
+// Adds the reflected velocities (calcModifiedVelocitySumKernel :235) and the
+// position corrections (calcPosModificationAmountKernel :276-281) of hits
+// [0, nh), in that order, all from the pre-container state (c, V).
+template <class T>
+__device__ __forceinline__ void mesh_accumulate(const uint32_t (&hits)[MESH_MAX_HITS], int nh, const V3<T>& c, T r,
+                                                const vec4_t<T>& V, T e, const MeshView& mvv, T& svx, T& svy, T& svz,
+                                                T& mx, T& my, T& mz) {
+  using A = Ar<T>;
+  const T* tri = static_cast<const T*>(mvv.tri);
+  const T* nrm = static_cast<const T*>(mvv.nrm);
   for (int h = 0; h < nh; ++h) {
     const uint32_t t = hits[h];
-    const T* tv = mv.tri + 9 * (size_t)t;
-    const T* tn = mv.nrm + 3 * (size_t)t;
+    const T* tv = tri + 9 * (size_t)t;
+    const T* tn = nrm + 3 * (size_t)t;
     const V3<T> n = {tn[0], tn[1], tn[2]};
     const T vn2 = A::mul(T(2), dot3<T>(V.x, V.y, V.z, n.x, n.y, n.z));
     svx = A::fma(e, A::fma(-vn2, n.x, V.x), svx);
@@ -198,8 +213,37 @@ __device__ void mesh_contacts(vec4_t<T>& P, vec4_t<T>& V, const SceneParams<T>& 
     my = A::fma(-sc, n.y, my);
     mz = A::fma(-sc, n.z, mz);
   }
-  if (nh > 0) {  // calcAveragedVelocityKernel: only particles with a hit
-    const T hc = (T)nh;
+}
+
+// Triangle container of one particle, CUDA semantics
+// (PolygonContainerCUDA.cpp:130-226): every hit triangle in ascending index.
+template <class T>
+__device__ void mesh_contacts(vec4_t<T>& P, vec4_t<T>& V, const SceneParams<T>& sp, const MeshView& mvv,
+                              uint32_t* err) {
+  using A = Ar<T>;
+  const T r = P.w;
+  const V3<T> c = {P.x, P.y, P.z};
+  // MESH_MAX_HITS hits per pass, in ascending triangle index: a sphere that
+  // touches more triangles takes further passes, each starting above the
+  // previous pass's largest id, so the sums come out as one ascending pass
+  // over every hit would give them.  The ids rise from pass to pass, so the
+  // passes end.
+  T svx = 0, svy = 0, svz = 0, mx = 0, my = 0, mz = 0;
+  uint32_t n_hits = 0;
+  uint32_t after = 0;  // ids <= after were applied by earlier passes
+  bool first = true;
+  for (;;) {
+    uint32_t hits[MESH_MAX_HITS];
+    int nh = 0;
+    const bool more = mesh_collect<T>(c, r, sp, mvv, err, first, after, hits, nh);
+    mesh_accumulate<T>(hits, nh, c, r, V, sp.e_poly, mvv, svx, svy, svz, mx, my, mz);
+    n_hits += (uint32_t)nh;
+    if (__builtin_expect(!more || nh == 0, 1)) break;
+    after = hits[nh - 1];
+    first = false;
+  }
+  if (n_hits > 0) {  // calcAveragedVelocityKernel: only particles with a hit
+    const T hc = (T)n_hits;
     V.x = A::div(svx, hc);
     V.y = A::div(svy, hc);
     V.z = A::div(svz, hc);

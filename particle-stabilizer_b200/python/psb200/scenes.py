@@ -259,6 +259,49 @@ def box_mesh_scene(n: int = 120, seed: int = 41) -> Scene:
                  tri=box_container(), name="box_mesh")
 
 
+def fan_floor_box(half: float = 0.05, height: float = 0.1, n_fan: int = 300) -> np.ndarray:
+    """Closed box [-half, half]^2 x [0, height] whose floor is a fan of
+    n_fan triangles around the floor's centre (every floor triangle has a
+    vertex at the origin); the other faces are two triangles each.  Normals
+    point out."""
+    box = box_container((-half, -half, 0.0), (half, half, height), n=1)
+    walls = box[~np.all(box[:, 2::3] == 0.0, axis=1)]
+    # perimeter points of the floor square, counter-clockwise from (-h, -h)
+    corners = np.array([[-half, -half], [half, -half], [half, half], [-half, half]])
+    per_side = n_fan // 4
+    pts = []
+    for k in range(4):
+        a, b = corners[k], corners[(k + 1) % 4]
+        for j in range(per_side):
+            pts.append(a + (b - a) * j / per_side)
+    pts = np.asarray(pts)
+    fan = []
+    for k in range(len(pts)):
+        p, q = pts[k], pts[(k + 1) % len(pts)]
+        # (origin, q, p): clockwise seen from above, so the normal points down (out)
+        fan.append([0.0, 0.0, 0.0, q[0], q[1], 0.0, p[0], p[1], 0.0])
+    tri = np.concatenate([np.asarray(fan), walls])
+    return tri.astype(np.float32).astype(np.float64)
+
+
+def fan_floor_scene(n_fan: int = 300, seed: int = 43) -> Scene:
+    """Spheres of radius 0.01 in a box whose floor is a fine triangle fan
+    (fan_floor_box): one sphere sits on the fan's centre 1e-5 deep, so it
+    touches all n_fan floor triangles at once; two more press on the fan
+    away from the centre and touch a few tens; a loose layer above falls.
+    Spring 2, dt 1e-4.  Density 1000."""
+    rng = np.random.default_rng(seed)
+    r = 0.01
+    low = np.array([[0.0, 0.0, r - 1e-5], [0.025, 0.0, r - 2e-4], [-0.02, 0.015, r - 1e-4]])
+    g = np.stack(np.meshgrid(np.arange(4), np.arange(4), np.arange(2), indexing="ij"), -1).reshape(-1, 3)
+    high = np.array([-0.036, -0.036, 0.045]) + g * 0.024 + rng.uniform(-0.001, 0.001, size=(len(g), 3))
+    pos = np.concatenate([low, high])
+    vel = np.concatenate([np.zeros((3, 3)), rng.normal(0, 0.05, size=(len(g), 3))])
+    st = _state(pos, vel, np.full(len(pos), r), 1000.0)
+    return Scene(st, (-0.05, -0.05, 0.0), (0.05, 0.05, 0.1), (0, 0, -9.8), (0.7,) * 6, 2.0, 0.5, 1e-4,
+                 tri=fan_floor_box(n_fan=n_fan), name="fan_floor")
+
+
 def funnel_wall_scene(n: int = 2000, seed: int = 7, coarse: bool = True, z_max: float = 1.05,
                       widen: bool = True) -> Scene:
     """Spheres (r 0.003) on rings just inside the funnel's cone wall at

@@ -6,10 +6,12 @@ compiled for sm_100a by `make -C oracle ref`):
     python tests/golden/make_golden_cuda.py OUTDIR [NAME,NAME,...]
 
 For two small box scenes whose dynamics stay tame (a jittered lattice and a
-soft contact-rich pile) and two triangle containers read from OBJ files (a
-closed triangulated box whose outer spheres touch its walls and floor, and
-spheres pressing on the cone wall of a coarse funnel, every centre inside
-the mesh AABB, which is the reference's grid domain), it records after
+soft contact-rich pile) and three triangle containers read from OBJ files
+(a closed triangulated box whose outer spheres touch its walls and floor,
+spheres pressing on the cone wall of a coarse funnel, and a box whose floor
+is a 300-triangle fan with one sphere touching every fan triangle at once;
+every centre inside the mesh AABB, which is the reference's grid domain),
+it records after
 several step counts the reference's bucket arrays (per-cell counts,
 exclusive offsets, particle index list) and its particle states.  The CPU
 tests pin the oracle's CUDA scheme to these, and the mesh fixtures its
@@ -77,6 +79,7 @@ SCENES = {
     "pile": lambda: scenes.pile(600, seed=51, k_spring=1.0),
     "mesh_box": lambda: scenes.box_mesh_scene(),
     "mesh_funnel": lambda: scenes.funnel_wall_scene(600, seed=17, z_max=0.95, widen=False),
+    "mesh_fan": lambda: scenes.fan_floor_scene(),
 }
 
 

@@ -74,7 +74,18 @@ def fixture_scene(g):
 
 def test_reference_cuda_fixtures_cover_both_containers():
     names = {os.path.basename(p) for p in CUDA_FIXTURES}
-    assert {"ref_cuda_lattice.npz", "ref_cuda_pile.npz", "ref_cuda_mesh_box.npz", "ref_cuda_mesh_funnel.npz"} <= names
+    assert {"ref_cuda_lattice.npz", "ref_cuda_pile.npz", "ref_cuda_mesh_box.npz", "ref_cuda_mesh_funnel.npz",
+            "ref_cuda_mesh_fan.npz"} <= names
+
+
+def test_reference_cuda_fan_fixture_has_a_sphere_on_every_fan_triangle():
+    """In the fan fixture the reference's container moved the centre sphere
+    by one 1e-5 correction per fan triangle: 300 hits in one step."""
+    g = np.load(os.path.join(GOLDEN, "ref_cuda_mesh_fan.npz"))
+    sc = fixture_scene(g)
+    lifted = O.pre_grid_state(sc, sc.state, "f64")[0, 2] - O.pre_grid_state(
+        sc.copy(tri=None, box_min=(-1, -1, -1), box_max=(1, 1, 2)), sc.state, "f64")[0, 2]
+    assert round(lifted / 1e-5) == 300
 
 
 @pytest.mark.parametrize("path", CUDA_FIXTURES, ids=[os.path.basename(p) for p in CUDA_FIXTURES])

@@ -115,3 +115,24 @@ def test_cli_resolves_overlaps_and_writes_obj(need_gpu, tmp_path):
     with open(obj_out) as f:
         assert f.readline() == "o Generated particles\n"
     obj_out.unlink()
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("quirk", [1, 0])
+@pytest.mark.parametrize("n_fan", [64, 68, 128, 132, 300])
+def test_sphere_touching_more_triangles_than_one_pass_holds(need_gpu, precision, quirk, n_fan):
+    """A sphere resting on the centre of a fan floor touches every fan
+    triangle at once.  The device keeps 64 hits per pass and takes further
+    passes for the rest, in ascending triangle order; the oracle sums every
+    hit in one ascending loop.  Fan sizes sit on either side of one and two
+    full passes."""
+    sc = scenes.fan_floor_scene(n_fan=n_fan).copy(edge_quirk=quirk)
+    # the oracle's own container pass: the centre sphere gets one 1e-5
+    # correction per hit, so its lift counts the hits
+    lifted = O.pre_grid_state(sc, sc.state, "f64")[0, 2] - O.pre_grid_state(
+        sc.copy(tri=None, box_min=(-1, -1, -1), box_max=(1, 1, 2)), sc.state, "f64")[0, 2]
+    assert round(lifted / 1e-5) == n_fan
+    for steps in (1, 30):
+        got = cast(run_gpu(sc, steps, precision), precision)
+        want = O.run(sc, steps, precision)
+        assert np.array_equal(got, want), f"{np.sum(np.any(got != want, axis=1))} of {sc.n} differ after {steps}"

@@ -130,6 +130,7 @@ def test_1000_step_trajectories_within_reference_run_to_run_spread(need_gpu):
 MESH_SCENES = {
     "box": lambda: scenes.box_mesh_scene(),
     "funnel": lambda: scenes.funnel_wall_scene(600, seed=17, z_max=0.95, widen=False),
+    "fan": lambda: scenes.fan_floor_scene(),
 }
 
 
@@ -141,8 +142,10 @@ def test_triangle_container_equals_reference_cuda(need_gpu, tmp_path, name, step
     (PolygonContainerCUDA::resolveCollisions, PolygonContainerCUDA.cpp:
     130-226, kernels PolygonContainerCUDA_kernels.cu:114-294), read from the
     same OBJ file: a closed triangulated box whose outer spheres touch its
-    walls and floor, and spheres pressing on the cone wall of a coarse
-    funnel.  Every centre starts inside the mesh AABB, the reference's grid
+    walls and floor, spheres pressing on the cone wall of a coarse funnel,
+    and a sphere touching all 300 triangles of a fan floor at once (the
+    reference keeps every hit; so must the bounded hit buffer here).  Every
+    centre starts inside the mesh AABB, the reference's grid
     domain.  Counts and offsets are compared exactly, bucket members as
     sets, states within FP64 rounding of the reference's atomic sums."""
     sc = MESH_SCENES[name]()
