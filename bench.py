@@ -462,7 +462,7 @@ EXTRAS = {
     "batch": lambda p, s, dev, a: batch_measure(p, s, dev, 100, 256, sequential=not a.no_sequential,
                                                 k_range=(0.25, 2.5), tune=True),
     "batch_as_specified": lambda p, s, dev, a: batch_measure(p, s, dev, 100, 256, sequential=not a.no_sequential),
-    "mesh": lambda p, s, dev, a: mesh_measure(p, s, dev, 20000),
+    "mesh": lambda p, s, dev, a: mesh_measure(p, s, dev, a.mesh_steps),
     "lists": lambda p, s, dev, a: lists_measure(p, s, dev, a.scene, a.skin),
 }
 
@@ -678,6 +678,8 @@ def main():
                     help="run only this secondary measurement on the local GPU and print its JSON")
     ap.add_argument("--no-sequential", action="store_true",
                     help="with --extra batch: skip the scene-by-scene comparison")
+    ap.add_argument("--mesh-steps", type=int, default=20000,
+                    help="steps of the funnel measurement (the mesh line; fewer for profiling runs)")
     ap.add_argument("--scene", default=None,
                     help="with --extra lists: measure only this scene (e.g. c2_1M_k0.25_fp32)")
     ap.add_argument("--skin", type=float, default=None,

@@ -131,7 +131,8 @@ struct SceneParams {
   uint32_t mesh_tris;
   uint32_t mesh_bin_base;  // first bin of this scene's triangle bins
   int32_t mesh_nb[3];      // triangle-bin grid
-  T mesh_lo[3];            // triangle-bin grid origin
+  T mesh_lo[3];            // triangle-bin grid origin = lower corner of the mesh AABB
+  T mesh_hi[3];            // upper corner of the mesh AABB
   T mesh_iv;               // triangle-bin edge
   int32_t edge_quirk;
   // unsigned division by nz and by ny with a multiply-high (Granlund &

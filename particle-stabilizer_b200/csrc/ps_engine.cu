@@ -89,7 +89,7 @@ struct GridHost {
   int32_t nb[3];
   int64_t n_cells, cbase;
   // triangle bins
-  double mesh_lo[3], mesh_iv;
+  double mesh_lo[3], mesh_hi[3], mesh_iv;
   int32_t mesh_nb[3];
   int64_t n_bins, bin_base, tri_base, n_tri;
 };
@@ -604,6 +604,7 @@ SceneParams<T> make_params(const ps_scene_desc& d, const GridHost& g, int64_t pb
     sp.nb[a] = g.nb[a];
     sp.mesh_nb[a] = g.mesh_nb[a];
     sp.mesh_lo[a] = (T)g.mesh_lo[a];
+    sp.mesh_hi[a] = (T)g.mesh_hi[a];
   }
   sp.interval = (T)g.interval;
   sp.e_lo[0] = (T)d.e_wall[PS_XMIN];
@@ -897,6 +898,7 @@ int size_grids(ps_sim* s, const double* aos) {
         }
       for (int a = 0; a < 3; ++a) {
         g.mesh_lo[a] = g.min[a];
+        g.mesh_hi[a] = g.max[a];
       }
       double ext = 0.0;
       for (int a = 0; a < 3; ++a) ext = std::max(ext, g.max[a] - g.min[a]);
@@ -926,6 +928,7 @@ int size_grids(ps_sim* s, const double* aos) {
         g.max[a] = d.box_max[a];
         g.mesh_nb[a] = 1;
         g.mesh_lo[a] = 0.0;
+        g.mesh_hi[a] = 0.0;
       }
       g.mesh_iv = 1.0;
     }

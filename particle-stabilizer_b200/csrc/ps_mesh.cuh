@@ -131,8 +131,14 @@ __device__ __forceinline__ bool mesh_collect(const V3<T>& c, T r, const ScenePar
   const int32_t bx0 = mesh_axis<T>(lox, sp.mesh_lo[0], sp.mesh_iv, sp.mesh_nb[0]);
   const int32_t by0 = mesh_axis<T>(loy, sp.mesh_lo[1], sp.mesh_iv, sp.mesh_nb[1]);
   const int32_t bz0 = mesh_axis<T>(loz, sp.mesh_lo[2], sp.mesh_iv, sp.mesh_nb[2]);
-  const int32_t bx1 = mesh_axis<T>(hix, sp.mesh_lo[0], sp.mesh_iv, sp.mesh_nb[0]);
   const int32_t by1 = mesh_axis<T>(hiy, sp.mesh_lo[1], sp.mesh_iv, sp.mesh_nb[1]);
+  // A sphere whose AABB misses the mesh AABB hits nothing: every triangle's
+  // AABB lies inside the mesh AABB (both from the same rounded vertices), so
+  // each closed AABB test would fail.  Such a sphere (above or beside the
+  // container) walks no bins.
+  const bool near = !(lox > sp.mesh_hi[0] || hix < sp.mesh_lo[0] || loy > sp.mesh_hi[1] || hiy < sp.mesh_lo[1] ||
+                      loz > sp.mesh_hi[2] || hiz < sp.mesh_lo[2]);
+  const int32_t bx1 = near ? mesh_axis<T>(hix, sp.mesh_lo[0], sp.mesh_iv, sp.mesh_nb[0]) : bx0 - 1;
   const int32_t bz1 = mesh_axis<T>(hiz, sp.mesh_lo[2], sp.mesh_iv, sp.mesh_nb[2]);
   nh = 0;
   bool more = false;
