@@ -189,6 +189,13 @@ void pdl_launch(void (*k)(KArgs...), unsigned g, unsigned blk, cudaStream_t st, 
   cudaLaunchKernelEx(&cfg, k, args...);
 }
 
+// The step scan for this simulation's grid size (tile of 2,048 or 8,192 cells).
+using StepScanFn = void (*)(const uint32_t*, uint32_t*, int64_t, const uint32_t*);
+StepScanFn step_scan_kernel(int64_t n) {
+  return step_scan_items(n) == STEP_SCAN_ITEMS_LARGE ? k_scan_with_tile_sums<STEP_SCAN_ITEMS_LARGE>
+                                                    : k_scan_with_tile_sums<STEP_SCAN_ITEMS_SMALL>;
+}
+
 template <class T>
 StepBufs<T> bufs(ps_sim* s) {
   StepBufs<T> b;
@@ -210,7 +217,8 @@ StepBufs<T> bufs(ps_sim* s) {
   b.tile_sum = s->tile_sum;
   b.scell = s->scell;
   b.bounds = static_cast<const T*>(s->d_bounds);
-  b.n_tiles = (uint32_t)scan_num_tiles(n_scan(s));
+  b.n_tiles = (uint32_t)step_scan_tiles(n_scan(s));
+  b.tile_shift = step_scan_shift(n_scan(s));
   b.n_scan = (uint32_t)n_scan(s);
   b.tape_p = nullptr;
   b.tape_v = nullptr;
@@ -279,7 +287,7 @@ int64_t enqueue_steps(ps_sim* s, int64_t steps) {
   const SceneParams<T> sp0 = params<T>(s)[0];
   const unsigned gb = blocks_for(s->n_total);
   const unsigned gp = blocks_for(s->n_total);
-  const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
+  const unsigned gs = (unsigned)step_scan_tiles(n_scan(s));
   cudaStream_t st = s->stream;
   int64_t launches = 0;
   const MeshView* mv = s->d_mesh_view;
@@ -288,7 +296,7 @@ int64_t enqueue_steps(ps_sim* s, int64_t steps) {
   pdl_launch(k_begin<T, MULTI, MESH, true>, gb, STEP_THREADS, st, b, sp0, mv);
   ++launches;
   for (int64_t k = 0; k < steps; ++k) {
-    pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, nsc,
+    pdl_launch(step_scan_kernel(n_scan(s)), gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, nsc,
                (const uint32_t*)s->tile_sum);
     pdl_launch(k_scatter, move_blocks(s->n_total, b.n_tiles), STEP_THREADS, st, (const uint32_t*)s->cell, s->slot,
                (const uint32_t*)s->orig, (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles, s->err);
@@ -317,7 +325,7 @@ void enqueue_steps_recorded(ps_sim* s, int64_t steps, std::vector<LaunchRecord>&
   const SceneParams<T> sp0 = params<T>(s)[0];
   const unsigned gb = blocks_for(s->n_total);
   const unsigned gp = blocks_for(s->n_total);
-  const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
+  const unsigned gs = (unsigned)step_scan_tiles(n_scan(s));
   cudaStream_t st = s->stream;
   size_t r = 0;
   auto pre = [&](int kind) {
@@ -330,7 +338,7 @@ void enqueue_steps_recorded(ps_sim* s, int64_t steps, std::vector<LaunchRecord>&
   post();
   for (int64_t k = 0; k < steps; ++k) {
     pre(PS_K_SCAN);
-    k_scan_with_tile_sums<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->tile_sum);
+    step_scan_kernel(n_scan(s))<<<gs, SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s), s->tile_sum);
     post();
     pre(PS_K_SCATTER);
     k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
@@ -403,7 +411,7 @@ cudaError_t enqueue_steps_list(ps_sim* s, int64_t steps) {
   const ListBufs<T> L = list_bufs<T>(s);
   const SceneParams<T> sp0 = params<T>(s)[0];
   const unsigned gp = blocks_for(s->n_total);
-  const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
+  const unsigned gs = (unsigned)step_scan_tiles(n_scan(s));
   const unsigned gm0 = move_blocks(s->n_total, b.n_tiles), gm1 = move_blocks(s->n_total, 0);
   cudaStream_t st = s->stream;
   const MeshView* mv = s->d_mesh_view;
@@ -413,7 +421,7 @@ cudaError_t enqueue_steps_list(ps_sim* s, int64_t steps) {
   cudaMemsetAsync(s->count, 0, sizeof(uint32_t) * (size_t)nsc, st);
   cudaMemsetAsync(s->tile_sum, 0, sizeof(uint32_t) * (size_t)b.n_tiles, st);
   pdl_launch(k_begin<T, MULTI, MESH, true>, gp, STEP_THREADS, st, b, sp0, mv);
-  pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, nsc,
+  pdl_launch(step_scan_kernel(n_scan(s)), gs, SCAN_THREADS, st, (const uint32_t*)s->count, s->offset, nsc,
              (const uint32_t*)s->tile_sum);
   pdl_launch(k_scatter, gm0, STEP_THREADS, st, (const uint32_t*)s->cell, s->slot, (const uint32_t*)s->orig,
              (const uint32_t*)s->offset, s->tmp, s->count, nt, s->tile_sum, b.n_tiles, s->err);
@@ -491,8 +499,9 @@ void enqueue_regrid(ps_sim* s) {
   const unsigned gp = blocks_for(s->n_total);
   cudaStream_t st = s->stream;
   k_begin<T, MULTI, false, false><<<gb, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
-  k_tile_sums<<<(unsigned)scan_num_tiles(n_scan(s)), STEP_THREADS, 0, st>>>(s->count, n_scan(s), s->tile_sum);
-  k_scan_with_tile_sums<<<(unsigned)scan_num_tiles(n_scan(s)), SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s),
+  k_tile_sums<<<(unsigned)step_scan_tiles(n_scan(s)), STEP_THREADS, 0, st>>>(s->count, n_scan(s), s->tile_sum,
+                                                                              step_scan_shift(n_scan(s)));
+  step_scan_kernel(n_scan(s))<<<(unsigned)step_scan_tiles(n_scan(s)), SCAN_THREADS, 0, st>>>(s->count, s->offset, n_scan(s),
                                                                                      s->tile_sum);
   k_scatter<<<move_blocks(s->n_total, b.n_tiles), STEP_THREADS, 0, st>>>(s->cell, s->slot, s->orig, s->offset, s->tmp,
                                                                        s->count, (uint32_t)s->n_total, s->tile_sum, b.n_tiles, s->err);
@@ -959,7 +968,7 @@ int size_grids(ps_sim* s, const double* aos) {
 
   // per-cell arrays and scan scratch
   const size_t cells_b = align_up(sizeof(uint32_t) * (size_t)(s->c_total + 1), 256);
-  const size_t tiles_b = align_up(sizeof(uint32_t) * (size_t)scan_num_tiles(n_scan(s)), 256);
+  const size_t tiles_b = align_up(sizeof(uint32_t) * (size_t)step_scan_tiles(n_scan(s)), 256);
   PS_CUDA(cudaMalloc(&s->cell_arena, 2 * cells_b + tiles_b));
   char* c = static_cast<char*>(s->cell_arena);
   s->count = reinterpret_cast<uint32_t*>(c);
@@ -1110,7 +1119,7 @@ int enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes, 
   StepBufs<T> b = bufs<T>(s);
   const SceneParams<T> sp0 = params<T>(s)[0];
   const unsigned gp = blocks_for(s->n_total);
-  const unsigned gs = (unsigned)scan_num_tiles(n_scan(s));
+  const unsigned gs = (unsigned)step_scan_tiles(n_scan(s));
   cudaStream_t st = s->stream;
   k_begin<T, MULTI, false, true><<<gp, STEP_THREADS, 0, st>>>(b, sp0, s->d_mesh_view);
   for (int64_t k = 0; k < steps; ++k) {
@@ -1120,7 +1129,7 @@ int enqueue_steps_taped(ps_sim* s, int64_t steps, char* tape, size_t row_bytes, 
     b.tape_o = row.o;
     uint32_t* off_k = offs + offs_stride * (size_t)k;
     b.offset = off_k;
-    pdl_launch(k_scan_with_tile_sums, gs, SCAN_THREADS, st, (const uint32_t*)s->count, off_k, n_scan(s),
+    pdl_launch(step_scan_kernel(n_scan(s)), gs, SCAN_THREADS, st, (const uint32_t*)s->count, off_k, n_scan(s),
                (const uint32_t*)s->tile_sum);
     pdl_launch(k_scatter, move_blocks(s->n_total, b.n_tiles), STEP_THREADS, st, (const uint32_t*)s->cell, s->slot,
                (const uint32_t*)s->orig, (const uint32_t*)off_k, s->tmp, s->count, (uint32_t)s->n_total,
@@ -1497,7 +1506,7 @@ int step_lists(ps_sim* s, int64_t n_steps) {
     const uint32_t rest = e & ~list_err;
     PS_CUDA(cudaMemcpyAsync(s->err, &rest, sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
     PS_CUDA(cudaMemsetAsync(s->count, 0, sizeof(uint32_t) * (size_t)n_scan(s), s->stream));
-    PS_CUDA(cudaMemsetAsync(s->tile_sum, 0, sizeof(uint32_t) * (size_t)scan_num_tiles(n_scan(s)), s->stream));
+    PS_CUDA(cudaMemsetAsync(s->tile_sum, 0, sizeof(uint32_t) * (size_t)step_scan_tiles(n_scan(s)), s->stream));
     PS_CUDA(cudaStreamSynchronize(s->stream));
     ++s->list_fallbacks;
     rc = load_state(s, s->list_ckpt);

@@ -208,12 +208,15 @@ __global__ void __launch_bounds__(STEP_THREADS) k_list_rebuild(StepBufs<T> b, Sc
   for (uint32_t base = blockIdx.x * STEP_THREADS; base < b.n; base += gridDim.x * STEP_THREADS) {
     const uint32_t p = base + threadIdx.x;
     const bool valid = p < b.n;
-    count_cell(b.count, b.tile_sum, valid ? b.cell[p] : 0u, valid);
+    count_cell(b.count, b.tile_sum, valid ? b.cell[p] : 0u, valid, b.tile_shift);
   }
   if (!grid_barrier(bar, b.err)) return;
   for (uint32_t t = blockIdx.x; t < scan_tiles; t += gridDim.x) {
     __syncthreads();  // the tile scan reuses its shared arrays
-    scan_tile_with_sums<true>(t, b.count, b.offset, n_cells, b.tile_sum);
+    if (b.tile_shift == 13u)
+      scan_tile_with_sums<true, STEP_SCAN_ITEMS_LARGE>(t, b.count, b.offset, n_cells, b.tile_sum);
+    else
+      scan_tile_with_sums<true, STEP_SCAN_ITEMS_SMALL>(t, b.count, b.offset, n_cells, b.tile_sum);
   }
   if (!grid_barrier(bar, b.err)) return;
   for (uint32_t blk = blockIdx.x; blk < scatter_blocks; blk += gridDim.x)

@@ -27,6 +27,26 @@ constexpr uint32_t SCAN_SPIN_LIMIT = 1u << 20;
 
 enum : uint32_t { SCAN_FLAG_NONE = 0, SCAN_FLAG_AGG = 1, SCAN_FLAG_PREFIX = 2 };
 
+// Tiles of the step scan (counts -> offsets with per-tile totals): 8,192
+// cells, or 2,048 for grids below STEP_SCAN_SMALL_BELOW cells, whose large
+// tiles would leave most SMs idle (the 110,592-cell lattice: scan 7.7 ->
+// 6.6 us; the 1.45 M-cell pile 10.4 -> 8.5 us; the 4.02 M-cell funnel and the
+// 7.95 M-cell box scene are as fast or faster with the large tile).
+constexpr int STEP_SCAN_ITEMS_LARGE = 32;
+constexpr int STEP_SCAN_ITEMS_SMALL = 8;
+constexpr int64_t STEP_SCAN_SMALL_BELOW = 2500000;
+__host__ __device__ inline int step_scan_items(int64_t n) {
+  return n < STEP_SCAN_SMALL_BELOW ? STEP_SCAN_ITEMS_SMALL : STEP_SCAN_ITEMS_LARGE;
+}
+__host__ __device__ inline uint32_t step_scan_shift(int64_t n) {  // log2 of the tile's cells
+  return step_scan_items(n) == STEP_SCAN_ITEMS_LARGE ? 13u : 11u;
+}
+__host__ __device__ inline int64_t step_scan_tiles(int64_t n) {
+  return (n + (int64_t(1) << step_scan_shift(n)) - 1) >> step_scan_shift(n);
+}
+static_assert(SCAN_THREADS * STEP_SCAN_ITEMS_LARGE == (1 << 13), "large step tile");
+static_assert(SCAN_THREADS * STEP_SCAN_ITEMS_SMALL == (1 << 11), "small step tile");
+
 // Scratch layout: [ticket (uint32) | spare uint32] [status words: one uint64 per tile].
 __host__ __device__ inline int64_t scan_num_tiles(int64_t n) { return (n + SCAN_TILE - 1) / SCAN_TILE; }
 __host__ __device__ inline size_t scan_scratch_bytes(int64_t n) { return 8 + 8 * (size_t)scan_num_tiles(n); }
@@ -177,16 +197,19 @@ __global__ void __launch_bounds__(SCAN_THREADS, 8) k_exclusive_scan_u32(const ui
 // carried from row to row; warps are combined through shared memory.
 // One CTA scans tile `tile`; a CTA that scans several tiles in turn
 // synchronises its threads between them.
-template <bool COH>
+// ITEMS elements per thread: STEP_SCAN_ITEMS_LARGE (8,192-cell tiles) for
+// large grids, STEP_SCAN_ITEMS_SMALL (2,048) where a grid would fill too few
+// CTAs with the large tile.
+template <bool COH, int ITEMS>
 __device__ __forceinline__ void scan_tile_with_sums(int64_t tile, const uint32_t* __restrict__ in,
                                                     uint32_t* __restrict__ out, int64_t n,
                                                     const uint32_t* __restrict__ tile_sum) {
-  constexpr int ROWS = SCAN_ITEMS / 4;  // uint4 per lane
+  constexpr int ROWS = ITEMS / 4;  // uint4 per lane
   __shared__ uint32_t s_warp[SCAN_THREADS / 32];
   __shared__ uint32_t s_pre[SCAN_THREADS / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-  const int64_t wbase = tile * SCAN_TILE + (int64_t)warp * (32 * SCAN_ITEMS);
+  const int64_t wbase = tile * (int64_t)(SCAN_THREADS * ITEMS) + (int64_t)warp * (32 * ITEMS);
 
   uint32_t pre = 0;
   for (int64_t t = tid; t < tile; t += SCAN_THREADS) pre += ld_ro<COH>(tile_sum + t);
@@ -194,7 +217,7 @@ __device__ __forceinline__ void scan_tile_with_sums(int64_t tile, const uint32_t
   for (int d = 16; d > 0; d >>= 1) pre += __shfl_xor_sync(0xffffffffu, pre, d);
   if (lane == 0) s_pre[warp] = pre;
 
-  const bool full = wbase + 32 * SCAN_ITEMS <= n;
+  const bool full = wbase + 32 * ITEMS <= n;
   uint4 v[ROWS];
 #pragma unroll
   for (int k = 0; k < ROWS; ++k) {
@@ -247,11 +270,12 @@ __device__ __forceinline__ void scan_tile_with_sums(int64_t tile, const uint32_t
   }
 }
 
+template <int ITEMS>
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_with_tile_sums(const uint32_t* __restrict__ in,
                                                                      uint32_t* __restrict__ out, int64_t n,
                                                                      const uint32_t* __restrict__ tile_sum) {
   pdl_wait();
-  scan_tile_with_sums<false>(blockIdx.x, in, out, n, tile_sum);
+  scan_tile_with_sums<false, ITEMS>(blockIdx.x, in, out, n, tile_sum);
 }
 
 }  // namespace psb

@@ -126,7 +126,8 @@ __device__ __forceinline__ void walls(vec4_t<T>& P, vec4_t<T>& V, const ScenePar
 // per tile) that the step's scan uses in place of a look-back.
 // With tile_sum null only the cell counts are taken (k_tile_sums forms the
 // totals afterwards).
-__device__ __forceinline__ void count_cell(uint32_t* count, uint32_t* tile_sum, uint32_t c, bool valid) {
+__device__ __forceinline__ void count_cell(uint32_t* count, uint32_t* tile_sum, uint32_t c, bool valid,
+                                           uint32_t tile_shift) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned active = __ballot_sync(0xffffffffu, valid);
   if (valid && tile_sum == nullptr) {
@@ -135,7 +136,7 @@ __device__ __forceinline__ void count_cell(uint32_t* count, uint32_t* tile_sum, 
   }
   if (valid) {
     atomicAdd(count + c, 1u);
-    const uint32_t t = c / (uint32_t)SCAN_TILE;
+    const uint32_t t = c >> tile_shift;
     const int first = __ffs(active) - 1;
     if (__all_sync(active, t == __shfl_sync(active, t, first))) {
       // the usual case in sorted order: the whole warp counts into one tile
@@ -165,7 +166,8 @@ struct StepBufs {
   int32_t n_scenes;
   uint32_t n;             // particles over all scenes
   uint32_t* tile_sum;     // per-tile totals of `count`, cleared by k_scatter
-  uint32_t n_tiles;
+  uint32_t n_tiles;       // tiles of the step scan
+  uint32_t tile_shift;    // log2 of a step-scan tile's cells
   uint32_t n_scan;        // entries of count and offset (cells over all scenes + 1)
   uint32_t* scell;        // global cell id of each sorted slot (written by k_rank_move)
   const T* bounds;        // per-scene, per-axis cell boundaries (see SceneParams::bnd_base)
@@ -222,16 +224,18 @@ __global__ void __launch_bounds__(STEP_THREADS) k_begin(StepBufs<T> b, ScenePara
   // A regrid (INTEGRATE false) hashes a state in any order, often the
   // upload's: per-tile totals would take one contended atomic per sphere, so
   // it counts cells only and k_tile_sums forms the totals.
-  count_cell(b.count, INTEGRATE ? b.tile_sum : nullptr, c, valid && in_bounds(c, b.n_scan - 1u, b.err));
+  count_cell(b.count, INTEGRATE ? b.tile_sum : nullptr, c, valid && in_bounds(c, b.n_scan - 1u, b.err), b.tile_shift);
 }
 
-// tile_sum[t] = sum of count over tile t (SCAN_TILE cells), one CTA per tile.
+// tile_sum[t] = sum of count over step-scan tile t (1 << tile_shift cells),
+// one CTA per tile.
 __global__ void __launch_bounds__(STEP_THREADS) k_tile_sums(const uint32_t* __restrict__ count, int64_t n,
-                                                           uint32_t* __restrict__ tile_sum) {
+                                                           uint32_t* __restrict__ tile_sum, uint32_t tile_shift) {
   __shared__ uint32_t s_red[STEP_THREADS / 32];
-  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+  const int64_t base = (int64_t)blockIdx.x << tile_shift;
+  const int64_t end = base + (int64_t(1) << tile_shift);
   uint32_t sum = 0;
-  for (int64_t e = base + threadIdx.x; e < base + SCAN_TILE && e < n; e += STEP_THREADS) sum += count[e];
+  for (int64_t e = base + threadIdx.x; e < end && e < n; e += STEP_THREADS) sum += count[e];
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, d);
   if ((threadIdx.x & 31u) == 0) s_red[threadIdx.x >> 5] = sum;
@@ -614,7 +618,7 @@ __global__ void __launch_bounds__(BLOCK, contact_min_blocks<T, BLOCK>()) k_conta
     }
   }
   if (FUSED) {
-    count_cell(b.count, b.tile_sum, c, valid && in_bounds(c, b.n_scan - 1u, b.err));
+    count_cell(b.count, b.tile_sum, c, valid && in_bounds(c, b.n_scan - 1u, b.err), b.tile_shift);
   }
 }
 
