@@ -11,14 +11,16 @@
 // the oracle), with the same operations as the reference:
 //   v <- mean over hits of e * (v - 2 (v.n) n)
 //   x <- x + sum over hits of -(r - dot(-n, x - v0)) n
-// all evaluated on the pre-container state.
+// all evaluated on the pre-container state.  A sphere may touch any number
+// of triangles: hits are kept MESH_MAX_HITS at a time, in passes over the
+// sphere's bins that each continue above the previous pass's largest id.
 #pragma once
 
 #include "ps_device.cuh"
 
 namespace psb {
 
-constexpr int MESH_MAX_HITS = 64;
+constexpr int MESH_MAX_HITS = 64;  // hits held per pass (more take further passes)
 
 // Device view of every scene's binned triangles.
 template <class T>
