@@ -122,8 +122,8 @@ __device__ __forceinline__ void walls(vec4_t<T>& P, vec4_t<T>& V, const ScenePar
 // does not wait for it; at a few particles per cell lanes rarely share a
 // cell, so aggregating them first costs more than it saves); the slot
 // inside the cell is taken later by k_scatter.  The same pass accumulates,
-// warp-aggregated, the per-tile totals of the count array (SCAN_TILE cells
-// per tile) that the step's scan uses in place of a look-back.
+// warp-aggregated, the per-tile totals of the count array (1 << tile_shift
+// cells per tile) that the step's scan uses in place of a look-back.
 // With tile_sum null only the cell counts are taken (k_tile_sums forms the
 // totals afterwards).
 __device__ __forceinline__ void count_cell(uint32_t* count, uint32_t* tile_sum, uint32_t c, bool valid,
