@@ -16,7 +16,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-ORACLE_SO = os.path.join(HERE, "_build", "libps_oracle.so")
+# PS_ORACLE_SO selects another build of the same sources (the sanitizer
+# build, oracle/_build_asan/, in tests/test_cpu_sanitizers.py)
+ORACLE_SO = os.environ.get("PS_ORACLE_SO") or os.path.join(HERE, "_build", "libps_oracle.so")
 REF_CPU_SO = os.path.join(HERE, "_ref", "libref_cpu.so")
 REF_CUDA_SO = os.path.join(HERE, "_ref", "libref_cuda.so")
 

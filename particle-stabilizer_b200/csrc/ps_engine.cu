@@ -31,12 +31,10 @@
 using namespace psb;
 
 // ---- error reporting ---------------------------------------------------------
-static thread_local std::string g_last_error;
+// The per-thread message behind ps_last_error() lives in host/ps_errors.cpp.
+extern "C" int ps_internal_fail(int code, const char* msg);
 
-static int fail(int code, const std::string& msg) {
-  g_last_error = msg;
-  return code;
-}
+static int fail(int code, const std::string& msg) { return ps_internal_fail(code, msg.c_str()); }
 
 #define PS_CUDA(expr)                                                                        \
   do {                                                                                       \
@@ -46,7 +44,6 @@ static int fail(int code, const std::string& msg) {
                   std::string(#expr) + ": " + cudaGetErrorString(e_));                      \
   } while (0)
 
-extern "C" const char* ps_last_error(void) { return g_last_error.c_str(); }
 
 extern "C" int32_t ps_bounds_checked(void) {
 #ifdef PS_DEBUG_BOUNDS
@@ -68,7 +65,6 @@ struct NvtxRange {
 };
 }  // namespace
 
-extern "C" int ps_internal_fail(int code, const char* msg) { return fail(code, msg ? msg : ""); }
 
 namespace {
 

@@ -81,6 +81,19 @@ class PSError(RuntimeError):
 _lib = None
 
 
+def declare_host(L: C.CDLL) -> None:
+    """Signatures of the host-side entry points (file formats,
+    post-processing, the error message): the part of the library that runs
+    without a GPU, also built alone with sanitizers (make host-asan)."""
+    L.ps_last_error.restype = C.c_char_p
+    L.ps_read_csv.argtypes = [C.c_char_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+    L.ps_write_csv.argtypes = [C.c_char_p, C.c_void_p, C.c_int64]
+    L.ps_read_obj.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+    L.ps_resolve_overlaps.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+    L.ps_overlap_stats.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+    L.ps_write_obj_spheres.argtypes = [C.c_char_p, C.c_void_p, C.c_int64]
+
+
 def lib() -> C.CDLL:
     """Load the CUDA library (raises if it has not been built)."""
     global _lib
@@ -88,7 +101,7 @@ def lib() -> C.CDLL:
         if not os.path.exists(LIB_PATH):
             raise PSError(f"{LIB_PATH} is missing: build it with `make -C particle-stabilizer_b200`")
         L = C.CDLL(LIB_PATH)
-        L.ps_last_error.restype = C.c_char_p
+        declare_host(L)
         L.ps_bounds_checked.restype = C.c_int32
         L.ps_create.argtypes = [C.POINTER(SceneDesc), C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
         L.ps_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
@@ -105,9 +118,6 @@ def lib() -> C.CDLL:
         L.ps_exclusive_scan_scratch_bytes.argtypes = [C.c_int64]
         L.ps_exclusive_scan_scratch_bytes.restype = C.c_size_t
         L.ps_exclusive_scan_u32.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
-        L.ps_read_csv.argtypes = [C.c_char_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
-        L.ps_write_csv.argtypes = [C.c_char_p, C.c_void_p, C.c_int64]
-        L.ps_read_obj.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
         L.ps_checkpoint_save.argtypes = [C.c_void_p, C.c_int32]
         L.ps_checkpoint_load.argtypes = [C.c_void_p, C.c_int32]
         L.ps_time_steps.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_double)]
@@ -120,10 +130,6 @@ def lib() -> C.CDLL:
         L.ps_list_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ps_tune_neighbor_lists.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                                              C.c_void_p]
-        L.ps_resolve_overlaps.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int64),
-                                          C.POINTER(C.c_double)]
-        L.ps_overlap_stats.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
-        L.ps_write_obj_spheres.argtypes = [C.c_char_p, C.c_void_p, C.c_int64]
         L.ps_set_contact_kernel.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
         L.ps_get_contact_kernel.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.ps_autotune.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
