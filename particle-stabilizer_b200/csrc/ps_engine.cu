@@ -34,7 +34,15 @@ using namespace psb;
 // The per-thread message behind ps_last_error() lives in host/ps_errors.cpp.
 extern "C" int ps_internal_fail(int code, const char* msg);
 
-static int fail(int code, const std::string& msg) { return ps_internal_fail(code, msg.c_str()); }
+// A runtime call that failed (an allocation the device cannot serve, say)
+// also leaves its error as this thread's "last error", which the next
+// cudaGetLastError returns: a later, unrelated call would report it again.
+// Reporting a CUDA failure therefore clears it (errors that break the
+// context stay sticky and keep being reported by the runtime itself).
+static int fail(int code, const std::string& msg) {
+  if (code == PS_ERR_CUDA || code == PS_ERR_NOMEM) (void)cudaGetLastError();
+  return ps_internal_fail(code, msg.c_str());
+}
 
 #define PS_CUDA(expr)                                                                        \
   do {                                                                                       \
