@@ -1904,6 +1904,10 @@ extern "C" int ps_backward(ps_sim* s, const double* dl_dstate, ps_grad* grads, d
   const NvtxRange nvtx_range("ps_backward");
   if (s == nullptr || dl_dstate == nullptr || grads == nullptr) return fail(PS_ERR_INVALID, "ps_backward: null argument");
   if (s->fwd_steps < 1) return fail(PS_ERR_INVALID, "ps_backward: call ps_forward_checkpointed first");
+  if (s->n_total == 0) {  // no particle: every gradient is zero
+    for (int sc = 0; sc < s->n_scenes; ++sc) grads[sc] = ps_grad{};
+    return PS_OK;
+  }
   DeviceGuard guard(s->device);
   ensure_l2_limit(s);
   if (s->precision == PS_FP32)
