@@ -127,3 +127,22 @@ def test_bounds_checked_build_exports_the_same_symbols():
     env["PYTHONPATH"] = os.pathsep.join([ROOT, os.path.join(ROOT, "particle-stabilizer_b200", "python")])
     r = subprocess.run(["python3", "-c", code], capture_output=True, text=True, env=env)
     assert r.returncode == 0 and "checked" in r.stdout, r.stderr
+
+
+C_PROGRAM = os.path.join(ROOT, "tests", "c_abi", "step_lattice.c")
+
+
+def build_c_program(out_dir):
+    """The header compiles as strict C11 and the program links against the
+    library (tests/c_abi/step_lattice.c, the C usage INTEGRATION.md shows)."""
+    exe = os.path.join(str(out_dir), "step_lattice")
+    lib_dir = os.path.dirname(psb200.LIB_PATH)
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"),
+                    C_PROGRAM, "-o", exe, "-L", lib_dir, "-lparticle_stabilizer_cuda", f"-Wl,-rpath,{lib_dir}"],
+                   check=True)
+    return exe
+
+
+def test_header_compiles_as_c_and_the_c_program_links(tmp_path):
+    exe = build_c_program(tmp_path)
+    assert os.access(exe, os.X_OK)
