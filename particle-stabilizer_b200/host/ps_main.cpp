@@ -112,7 +112,11 @@ int main(int argc, char** argv) {
   }
   if (a.fp32) setenv("PSB200_PRECISION", "fp32", 1);
   if (a.widen) setenv("PSB200_WIDEN_DOMAIN", "1", 1);
-  if (a.cellSize > 0) setenv("PSB200_CELL_SIZE", std::to_string(a.cellSize).c_str(), 1);
+  if (a.cellSize > 0) {  // all 17 digits, so the library reads back the same double
+    char buf[32];
+    std::snprintf(buf, sizeof buf, "%.17g", a.cellSize);
+    setenv("PSB200_CELL_SIZE", buf, 1);
+  }
 
   void* h = dlopen(a.libPath.c_str(), RTLD_LAZY);
   if (h == nullptr) {

@@ -136,3 +136,54 @@ def test_sphere_touching_more_triangles_than_one_pass_holds(need_gpu, precision,
         got = cast(run_gpu(sc, steps, precision), precision)
         want = O.run(sc, steps, precision)
         assert np.array_equal(got, want), f"{np.sum(np.any(got != want, axis=1))} of {sc.n} differ after {steps}"
+
+
+def write_xyzr_csv(path, state):
+    with open(path, "w") as f:
+        f.write("x,y,z,r\n")
+        for p in state:
+            f.write("%.17g,%.17g,%.17g,%.17g\n" % (p[0], p[1], p[2], p[6]))
+
+
+@pytest.mark.parametrize("flags", ["fp32", "cell_size", "widen_fp32", "zero_steps"])
+def test_cli_extra_flags(need_gpu, tmp_path, flags):
+    """The CLI's own flags reach the library unchanged: --fp32, --cell-size
+    (a value with more than six significant digits), --widen-domain (the
+    funnel, spheres above its rim), and --max-steps 0, which takes one step
+    as the reference's loop does.  The CSV equals the oracle's state written
+    by the same writer."""
+    funnel = flags == "widen_fp32"
+    sc = scenes.funnel_wall_scene(400, seed=21, z_max=1.05, widen=True) if funnel else scenes.pile(300, seed=23,
+                                                                                                   k_spring=1.0)
+    csv_in, csv_out = tmp_path / "in.csv", tmp_path / "out.csv"
+    write_xyzr_csv(csv_in, sc.state)
+    steps = 0 if flags == "zero_steps" else 20
+    cmd = [psb200.CLI_PATH, "--lib", psb200.LIB_PATH, str(csv_in), "--cuda", "--max-steps", str(steps),
+           "--dt", repr(sc.dt), "--coeff-of-spring", repr(sc.k_spring), "--coeff-of-restitution-sphere",
+           repr(sc.e_sphere), "--coeff-of-restitution-wall", *[repr(e) for e in sc.e_wall],
+           "--gravity", *map(repr, sc.gravity), "--initial-velocity", "0.1", "-0.2", "0.05", "--density", "1000",
+           "--out-csv-path", str(csv_out)]
+    if funnel:
+        obj = tmp_path / "funnel.obj"
+        scenes.write_obj(str(obj), sc.tri)
+        cmd += ["--container", str(obj), "--widen-domain", "--fp32"]
+    else:
+        cmd += ["--box-min", *map(repr, sc.box_min), "--box-max", *map(repr, sc.box_max)]
+    want_sc = sc
+    prec = "f64"
+    if flags == "fp32":
+        cmd.append("--fp32")
+        prec = "f32"
+    if funnel:
+        prec = "f32"
+    if flags == "cell_size":
+        cell = 2.1 * sc.r_max() * 1.2345678901
+        cmd += ["--cell-size", repr(cell)]
+        want_sc = sc.copy(interval=cell)
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    start = psb200.read_csv(str(csv_in), (0.1, -0.2, 0.05), 1000.0)
+    want = O.run(want_sc.copy(state=start), max(steps, 1), prec).astype(np.float64)
+    ref_csv = tmp_path / "want.csv"
+    psb200.write_csv(str(ref_csv), want)
+    assert csv_out.read_text() == ref_csv.read_text()
