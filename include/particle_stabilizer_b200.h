@@ -317,6 +317,18 @@ int ps_read_csv(const char* path, const double velocity[3], double density, doub
                 int64_t* n_out);
 int ps_write_csv(const char* path, const double* aos, int64_t n);
 
+/* Binary state file for checkpoint / resume.  No counterpart in the
+ * reference: its CSV output keeps positions and radii only, so a run cannot
+ * be continued from it.  This file keeps every particle record in full
+ * (8 doubles: x, y, z, vx, vy, vz, radius, mass, original order) and the
+ * number of steps taken, so a run resumed from it continues bit for bit.
+ * Layout, little-endian: 8-byte magic "PSB2STAT", uint32 version (1),
+ * uint32 0, int64 n, int64 steps, then 8*n doubles.
+ * ps_read_state_bin returns the record count in *n_out and fills at most
+ * `cap` records (aos_out may be NULL to query the count). */
+int ps_write_state_bin(const char* path, const double* aos, int64_t n, int64_t steps);
+int ps_read_state_bin(const char* path, double* aos_out, int64_t cap, int64_t* n_out, int64_t* steps_out);
+
 /* OBJ container file (PolygonContainerCUDA::readFromFile,
  * PolygonContainerCUDA.cpp:314-350): triangles de-indexed to 9 doubles each,
  * vertices read in single precision as assimp's default ai_real. */

@@ -4,11 +4,14 @@
 //                  (src/ParticleStabilizer/ParticleIO.cpp:39-144)
 //   OBJ container  PolygonContainerCUDA::readFromFile + de-indexing
 //                  (src/ParticleStabilizerCUDA/PolygonContainerCUDA.cpp:26-53, 314-350)
+//   state file     binary checkpoint / resume (every record and the step
+//                  count; no counterpart in the reference)
 //
 // Differences from the reference, by design: a malformed number makes the
 // reader return PS_ERR_IO (std::stod would throw and abort the reference),
 // and the OBJ reader is a self-contained triangle/polygon reader instead of
 // assimp (n-gons are fanned from their first vertex).
+#include <algorithm>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -107,6 +110,59 @@ extern "C" int ps_write_csv(const char* path, const double* aos, int64_t n) {
   }
   file.close();
   return file ? PS_OK : io_fail(std::string("write failed: ") + path);
+}
+
+namespace {
+constexpr char kStateMagic[8] = {'P', 'S', 'B', '2', 'S', 'T', 'A', 'T'};
+constexpr uint32_t kStateVersion = 1;
+}  // namespace
+
+extern "C" int ps_write_state_bin(const char* path, const double* aos, int64_t n, int64_t steps) {
+  if (path == nullptr || (aos == nullptr && n > 0) || n < 0 || steps < 0)
+    return io_fail("ps_write_state_bin: bad argument");
+  std::error_code ec;
+  const std::filesystem::path dir = std::filesystem::absolute(path).parent_path();
+  if (!std::filesystem::exists(dir)) std::filesystem::create_directories(dir, ec);
+  std::ofstream file(path, std::ios::binary);
+  if (!file) return io_fail(std::string("Could not open file ") + path);
+  const uint32_t version = kStateVersion, zero = 0;
+  file.write(kStateMagic, sizeof kStateMagic);
+  file.write(reinterpret_cast<const char*>(&version), sizeof version);
+  file.write(reinterpret_cast<const char*>(&zero), sizeof zero);
+  file.write(reinterpret_cast<const char*>(&n), sizeof n);
+  file.write(reinterpret_cast<const char*>(&steps), sizeof steps);
+  if (n > 0) file.write(reinterpret_cast<const char*>(aos), (std::streamsize)(8 * sizeof(double) * (size_t)n));
+  file.close();
+  return file ? PS_OK : io_fail(std::string("write failed: ") + path);
+}
+
+extern "C" int ps_read_state_bin(const char* path, double* aos_out, int64_t cap, int64_t* n_out, int64_t* steps_out) {
+  if (path == nullptr || n_out == nullptr || cap < 0) return io_fail("ps_read_state_bin: bad argument");
+  std::ifstream file(path, std::ios::binary);
+  if (!file.is_open()) return io_fail(std::string("Could not open file: ") + path);
+  char magic[8];
+  uint32_t version = 0, zero = 0;
+  int64_t n = -1, steps = -1;
+  file.read(magic, sizeof magic);
+  file.read(reinterpret_cast<char*>(&version), sizeof version);
+  file.read(reinterpret_cast<char*>(&zero), sizeof zero);
+  file.read(reinterpret_cast<char*>(&n), sizeof n);
+  file.read(reinterpret_cast<char*>(&steps), sizeof steps);
+  if (!file || std::memcmp(magic, kStateMagic, sizeof magic) != 0 || version != kStateVersion || n < 0 || steps < 0)
+    return io_fail(std::string("ps_read_state_bin: not a state file (version 1): ") + path);
+  file.seekg(0, std::ios::end);
+  const std::streamoff payload = file.tellg() - (std::streamoff)(sizeof magic + 2 * sizeof(uint32_t) + 2 * sizeof(int64_t));
+  if (payload != (std::streamoff)(8 * sizeof(double)) * n)
+    return io_fail(std::string("ps_read_state_bin: truncated or oversized file: ") + path);
+  if (aos_out != nullptr && cap > 0 && n > 0) {
+    file.seekg((std::streamoff)(sizeof magic + 2 * sizeof(uint32_t) + 2 * sizeof(int64_t)), std::ios::beg);
+    const int64_t m = std::min(n, cap);
+    file.read(reinterpret_cast<char*>(aos_out), (std::streamsize)(8 * sizeof(double) * (size_t)m));
+    if (!file) return io_fail(std::string("ps_read_state_bin: read failed: ") + path);
+  }
+  *n_out = n;
+  if (steps_out != nullptr) *steps_out = steps;
+  return PS_OK;
 }
 
 extern "C" int ps_read_obj(const char* path, double* tri_out, int64_t cap, int64_t* n_tri_out) {

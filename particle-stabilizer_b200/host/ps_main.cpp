@@ -6,7 +6,9 @@
 // runSimulateCUDA symbol (ParticleStabilizerMain.cpp:19-21,235-256).  The
 // reference's CPU simulator is not part of this program: the B200 path runs
 // whether or not --cuda is given.  Extra flags: --fp32 (single precision),
-// --cell-size S, --widen-domain, --lib PATH.  --visualize has no graphics
+// --cell-size S, --widen-domain, --lib PATH, and --dump-state /
+// --resume-state (a binary file with every particle record and the step
+// count, which the reference's CSV cannot give).  --visualize has no graphics
 // stack to open and is reported and skipped.  After the run, as the
 // reference (ParticleStabilizerMain.cpp:274-296): --resolve-overlap-axis
 // (ps_resolve_overlaps), then the CSV, then --out-obj-path
@@ -32,11 +34,14 @@ using write_csv_t = int (*)(const char*, const double*, int64_t);
 using resolve_t = int (*)(double*, int64_t, int32_t, int64_t*, double*);
 using write_obj_t = int (*)(const char*, const double*, int64_t);
 using last_error_t = const char* (*)();
+using write_state_t = int (*)(const char*, const double*, int64_t, int64_t);
+using read_state_t = int (*)(const char*, double*, int64_t, int64_t*, int64_t*);
 
 namespace {
 
 struct Args {
   std::string particleFilePath, objOutPath, particleOutPath, containerPath, libPath = "./libparticle_stabilizer_cuda.so";
+  std::string dumpStatePath, resumeStatePath;  // binary state files (checkpoint / resume)
   dvec3 initialVelocity{0.0, 0.0, -10.0};
   double density = 1.0;
   CoefficientOfRestitutionWall e_wall{0.5, 0.5, 0.5, 0.5, 0.5, 0.5};
@@ -58,7 +63,9 @@ void usage() {
                "  --coeff-of-spring SPRING  --coeff-of-restitution-sphere E  --gravity X Y Z\n"
                "  --dt DT  --max-steps N  --box-min X Y Z  --box-max X Y Z  --container OBJ\n"
                "  --out-csv-path CSV  --out-obj-path OBJ  --resolve-overlap-axis AXIS  --visualize\n"
-               "  --fp32  --cell-size S  --widen-domain  --lib PATH\n";
+               "  --fp32  --cell-size S  --widen-domain  --lib PATH\n"
+               "  --dump-state BIN    after the run, write every particle record and the step count\n"
+               "  --resume-state BIN  start from a dumped state (the particle file is then optional)\n";
 }
 
 bool parse(int argc, char** argv, Args& a) {
@@ -97,9 +104,11 @@ bool parse(int argc, char** argv, Args& a) {
     else if (s == "--cell-size") { need(i, 1); a.cellSize = std::stod(argv[++i]); }
     else if (s == "--widen-domain") a.widen = true;
     else if (s == "--lib") { need(i, 1); a.libPath = argv[++i]; }
+    else if (s == "--dump-state") { need(i, 1); a.dumpStatePath = argv[++i]; }
+    else if (s == "--resume-state") { need(i, 1); a.resumeStatePath = argv[++i]; }
     else a.particleFilePath = s;
   }
-  return !a.particleFilePath.empty();
+  return !a.particleFilePath.empty() || !a.resumeStatePath.empty();
 }
 
 }  // namespace
@@ -135,16 +144,36 @@ int main(int argc, char** argv) {
   }
   if (!a.toUseCUDA) std::cout << "[info] this program runs the B200 path (--cuda implied)\n";
 
-  // ParticleData::readFromCSV (ParticleIO.cpp:90-144)
-  const double vel[3] = {a.initialVelocity.x, a.initialVelocity.y, a.initialVelocity.z};
-  int64_t n = 0;
-  if (read_csv(a.particleFilePath.c_str(), vel, a.density, nullptr, 0, &n) != PS_OK) {
-    std::cerr << "[critical] " << last_error() << "\n";
+  auto write_state = reinterpret_cast<write_state_t>(dlsym(h, "ps_write_state_bin"));
+  auto read_state = reinterpret_cast<read_state_t>(dlsym(h, "ps_read_state_bin"));
+  if ((!a.dumpStatePath.empty() || !a.resumeStatePath.empty()) && (!write_state || !read_state)) {
+    std::cerr << "Cannot load symbol: 'ps_write_state_bin' from the shared library.\n";
     return EXIT_FAILURE;
   }
-  std::vector<double> aos((size_t)(8 * n));
-  read_csv(a.particleFilePath.c_str(), vel, a.density, aos.data(), n, &n);
-  std::cout << "[info] Read " << n << " particles from file: " << a.particleFilePath << "\n";
+
+  int64_t n = 0, steps_before = 0;
+  std::vector<double> aos;
+  if (!a.resumeStatePath.empty()) {
+    // every record in full (velocities included) and the steps already taken
+    if (read_state(a.resumeStatePath.c_str(), nullptr, 0, &n, &steps_before) != PS_OK) {
+      std::cerr << "[critical] " << last_error() << "\n";
+      return EXIT_FAILURE;
+    }
+    aos.resize((size_t)(8 * n));
+    read_state(a.resumeStatePath.c_str(), aos.data(), n, &n, &steps_before);
+    std::cout << "[info] Resumed " << n << " particles after " << steps_before << " steps from file: "
+              << a.resumeStatePath << "\n";
+  } else {
+    // ParticleData::readFromCSV (ParticleIO.cpp:90-144)
+    const double vel[3] = {a.initialVelocity.x, a.initialVelocity.y, a.initialVelocity.z};
+    if (read_csv(a.particleFilePath.c_str(), vel, a.density, nullptr, 0, &n) != PS_OK) {
+      std::cerr << "[critical] " << last_error() << "\n";
+      return EXIT_FAILURE;
+    }
+    aos.resize((size_t)(8 * n));
+    read_csv(a.particleFilePath.c_str(), vel, a.density, aos.data(), n, &n);
+    std::cout << "[info] Read " << n << " particles from file: " << a.particleFilePath << "\n";
+  }
 
   std::vector<ParticlePtr> particles;
   particles.reserve((size_t)n);
@@ -162,6 +191,14 @@ int main(int argc, char** argv) {
     q[0] = p.position.x; q[1] = p.position.y; q[2] = p.position.z;
     q[3] = p.velocity.x; q[4] = p.velocity.y; q[5] = p.velocity.z;
     q[6] = p.radius; q[7] = p.mass;
+  }
+  if (!a.dumpStatePath.empty()) {  // before any post-processing: the state a resumed run continues from
+    const int64_t steps = steps_before + (a.maxSteps == 0 ? 1 : a.maxSteps);  // the loop takes at least one step
+    if (write_state(a.dumpStatePath.c_str(), aos.data(), n, steps) != PS_OK) {
+      std::cerr << "[error] " << last_error() << "\n";
+      return EXIT_FAILURE;
+    }
+    std::cout << "[info] Wrote the state after " << steps << " steps to file " << a.dumpStatePath << "\n";
   }
   if (a.resolveOverlapAxis >= 0) {  // ParticleModel::resolveOverlaps (ParticleModel.cpp:154-259)
     std::cout << "[info] ### Resolving overlaps\n";

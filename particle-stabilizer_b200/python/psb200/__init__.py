@@ -32,7 +32,7 @@ EXPORTED = (
     "ps_checkpoint_save", "ps_checkpoint_load", "ps_time_steps", "ps_profile_steps", "ps_forward_checkpointed",
     "ps_backward", "ps_exclusive_scan_u32_noalloc", "ps_exclusive_scan_u32_noalloc_status", "ps_autotune", "ps_set_contact_kernel", "ps_get_contact_kernel", "ps_set_neighbor_lists", "ps_list_stats", "ps_tune_neighbor_lists",
     "ps_resolve_overlaps", "ps_overlap_stats",
-    "ps_write_obj_spheres", "ps_bounds_checked", "runSimulateCUDA",
+    "ps_write_obj_spheres", "ps_bounds_checked", "ps_write_state_bin", "ps_read_state_bin", "runSimulateCUDA",
 )
 KERNEL_KINDS = ("begin", "scan", "scatter", "rank_move", "contacts")
 
@@ -92,6 +92,8 @@ def declare_host(L: C.CDLL) -> None:
     L.ps_resolve_overlaps.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     L.ps_overlap_stats.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     L.ps_write_obj_spheres.argtypes = [C.c_char_p, C.c_void_p, C.c_int64]
+    L.ps_write_state_bin.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.c_int64]
+    L.ps_read_state_bin.argtypes = [C.c_char_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
 
 
 def lib() -> C.CDLL:
@@ -412,6 +414,22 @@ def read_csv(path: str, velocity=(0.0, 0.0, -10.0), density: float = 1.0) -> np.
 def write_csv(path: str, state: np.ndarray) -> None:
     st = np.ascontiguousarray(state, dtype=np.float64)
     _check(lib().ps_write_csv(path.encode(), _ptr(st), st.shape[0]), "ps_write_csv")
+
+
+def write_state_bin(path: str, state: np.ndarray, steps: int = 0) -> None:
+    """ps_write_state_bin: every particle record (n x 8) and the step count."""
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    _check(lib().ps_write_state_bin(path.encode(), _ptr(st), st.shape[0], int(steps)), "ps_write_state_bin")
+
+
+def read_state_bin(path: str):
+    """ps_read_state_bin: (state n x 8, step count)."""
+    n, steps = C.c_int64(), C.c_int64()
+    _check(lib().ps_read_state_bin(path.encode(), None, 0, C.byref(n), C.byref(steps)), "ps_read_state_bin")
+    out = np.empty((n.value, 8), dtype=np.float64)
+    _check(lib().ps_read_state_bin(path.encode(), _ptr(out), n.value, C.byref(n), C.byref(steps)),
+           "ps_read_state_bin")
+    return out, int(steps.value)
 
 
 def read_obj(path: str) -> np.ndarray:

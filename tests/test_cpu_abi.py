@@ -146,3 +146,33 @@ def build_c_program(out_dir):
 def test_header_compiles_as_c_and_the_c_program_links(tmp_path):
     exe = build_c_program(tmp_path)
     assert os.access(exe, os.X_OK)
+
+
+def test_state_file_round_trip_and_bad_files(tmp_path):
+    """ps_write_state_bin / ps_read_state_bin keep every record bit for bit
+    (signed zeros, subnormals, infinities and NaN payloads included) and the
+    step count; files that are not state files, or are cut short, are
+    errors, not garbage."""
+    rng = np.random.default_rng(5)
+    st = rng.normal(size=(257, 8))
+    st[0, :4] = [-0.0, 5e-324, np.inf, -np.inf]
+    st[1, 0] = np.frombuffer(np.uint64(0x7FF8_0000_0000_1234).tobytes(), dtype=np.float64)[0]  # a NaN payload
+    p = tmp_path / "sub" / "s.bin"  # the writer creates missing directories
+    psb200.write_state_bin(str(p), st, 12345)
+    got, steps = psb200.read_state_bin(str(p))
+    assert steps == 12345 and got.tobytes() == st.tobytes()
+    assert os.path.getsize(p) == 32 + 64 * st.shape[0]
+    empty = tmp_path / "e.bin"
+    psb200.write_state_bin(str(empty), np.zeros((0, 8)), 0)
+    got, steps = psb200.read_state_bin(str(empty))
+    assert got.shape == (0, 8) and steps == 0
+    cut = tmp_path / "cut.bin"
+    cut.write_bytes(p.read_bytes()[:-8])
+    with pytest.raises(psb200.PSError, match="truncated"):
+        psb200.read_state_bin(str(cut))
+    csv = tmp_path / "x.csv"
+    csv.write_text("x,y,z,r\n1,2,3,4\n")
+    with pytest.raises(psb200.PSError, match="not a state file"):
+        psb200.read_state_bin(str(csv))
+    with pytest.raises(psb200.PSError, match="Could not open"):
+        psb200.read_state_bin(str(tmp_path / "missing.bin"))
