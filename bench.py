@@ -45,11 +45,11 @@ UNIT = "particle-steps/s"
 WORKLOAD = ("1,048,576 spheres, log-normal r (median 0.002, sigma 0.25, clip [0.001,0.004]), box 1x1x4, "
             "k 5e4, e 0.4, walls 0.7, dt 5e-6, cell 2 r_max")
 L2_BYTES = 126 * 2 ** 20
-# DRAM bytes per launch of the fused FP32 contacts kernel on this workload,
-# measured with ncu in steady state (--cache-control none, the second of two
-# captured launches: 38.7 MB read + 53.3 MB written; the algorithmic bytes
-# are 75.5 MB).
-CONTACTS_TRAFFIC = 91.97e6
+# DRAM bytes per launch of the fused FP32 contacts kernel (adaptive walk, the
+# default) on this workload, measured with ncu in steady state
+# (--cache-control none, the second of two captured launches: 35.2 MB read +
+# 50.9 MB written; the algorithmic bytes are 75.5 MB).
+CONTACTS_TRAFFIC = 86.09e6
 
 
 def peaks():

@@ -203,9 +203,10 @@ int ps_backward(ps_sim* sim, const double* dl_dstate, ps_grad* grads, double* dl
  * contacts, so later trajectories are those of the chosen grid: deterministic,
  * and equal to the oracle's with that cell size, but not bit-equal to runs
  * with the previous grid.  A recorded ps_forward_checkpointed is dropped.
- * Then, on the chosen grid and L, it times the four contact kernels
- * (PS_WALK_LANE with 128, 256 and 512 threads per CTA, PS_WALK_WARP with
- * 256) and keeps the fastest; they give identical results.
+ * Then, on the chosen grid and L, it times the five contact kernels
+ * (PS_WALK_LANE with 128, 256 and 512 threads per CTA, PS_WALK_WARP and
+ * PS_WALK_ADAPTIVE with 256) and keeps the fastest; they give identical
+ * results.
  * Allocates device memory (grids, graphs, one state copy). */
 /* ---- neighbour-list mode (no counterpart in the reference, which rebuilds
  * its grid every step, ParticleModelCUDA.cpp:115-155) ----
@@ -242,11 +243,11 @@ typedef struct ps_tune_result {
   double ms_per_step;        /* trial time per step with the choice               */
   double before_ms_per_step; /* trial time per step with the grid, L and contact  */
                              /* kernel in effect when ps_autotune was called      */
-  int32_t contact_walk;      /* chosen contact kernel: PS_WALK_LANE / PS_WALK_WARP */
+  int32_t contact_walk;      /* chosen contact kernel: PS_WALK_LANE/_WARP/_ADAPTIVE */
   int32_t contact_block;     /* and its threads per CTA                           */
-  double contact_ms[4];      /* ms per step, with the chosen f and L, of the      */
+  double contact_ms[5];      /* ms per step, with the chosen f and L, of the      */
                              /* contact kernels LANE/128, LANE/256, LANE/512,     */
-                             /* WARP/256                                          */
+                             /* WARP/256, ADAPTIVE/256                            */
 } ps_tune_result;
 int ps_autotune(ps_sim* sim, int64_t trial_steps, const double* cell_factors, int32_t n_factors,
                 const int64_t* graph_blocks, int32_t n_blocks, double* ms_table, ps_tune_result* out);
@@ -259,12 +260,19 @@ int ps_autotune(ps_sim* sim, int64_t trial_steps, const double* cell_factors, in
  * PS_WALK_WARP: each warp reads the union of its 32 spheres' candidates in
  * a neighbour column with coalesced loads and hands them to the lanes by
  * register shuffle; 256 threads per CTA (measured slower than the lane walk
- * on every scene tried; kept as a tuner candidate).  Every variant applies
+ * on every scene tried; kept as a tuner candidate).  PS_WALK_ADAPTIVE:
+ * each warp chooses, from its spheres' range lengths, between the per-lane
+ * walk and a flattened one (one loop over the concatenation of a thread's
+ * non-empty ranges, so the warp waits for as many candidate loads as its
+ * busiest lane has in all, not for the busiest lane of every column in
+ * turn); the flattened walk wins on sparse grids, the per-lane walk on
+ * dense piles; 256 threads.  Every variant applies
  * the same candidates in the same order, so results are bit-identical;
- * only the speed differs.  The default is PS_WALK_LANE with 256 threads.
+ * only the speed differs.  The default is PS_WALK_ADAPTIVE with 256 threads.
  * Changing it drops the captured step graphs. */
 #define PS_WALK_LANE 0
 #define PS_WALK_WARP 1
+#define PS_WALK_ADAPTIVE 2
 int ps_set_contact_kernel(ps_sim* sim, int32_t walk, int32_t block);
 int ps_get_contact_kernel(ps_sim* sim, int32_t* walk, int32_t* block);
 

@@ -141,8 +141,8 @@ struct ps_sim {
 
   std::map<int64_t, cudaGraphExec_t> graphs;
   int64_t graph_block = 200;  // steps per captured CUDA graph (ps_autotune may change it)
-  int32_t walk = WALK_LANE;   // neighbour walk of the contact kernel (WALK_LANE / WALK_WARP)
-  int32_t contact_block = 256;  // threads per CTA of the contact kernel (WALK_LANE: 128, 256, 512; WALK_WARP: 256)
+  int32_t walk = WALK_ADAPTIVE;  // neighbour walk of the contact kernel (WALK_LANE / WALK_WARP / WALK_ADAPTIVE)
+  int32_t contact_block = 256;    // threads per CTA of the contact kernel (WALK_LANE: 128, 256, 512; others: 256)
   int64_t last_launches = 0;
   std::map<int32_t, void*> checkpoints;  // slot -> device copy of (P0, V1, orig)
   cudaAccessPolicyWindow l2_window{};     // count + offset arrays kept in L2
@@ -251,13 +251,14 @@ unsigned move_blocks(int64_t n, uint32_t words) {
   return (unsigned)std::max<int64_t>((n + per - 1) / per, (words + STEP_THREADS - 1) / STEP_THREADS);
 }
 
-static_assert(WALK_LANE == PS_WALK_LANE && WALK_WARP == PS_WALK_WARP, "walk ids of the C ABI");
+static_assert(WALK_LANE == PS_WALK_LANE && WALK_WARP == PS_WALK_WARP && WALK_ADAPTIVE == PS_WALK_ADAPTIVE,
+              "walk ids of the C ABI");
 
 // Contact kernel variants the tuner times: {walk, threads per CTA}, in the
 // order of ps_tune_result::contact_ms.
-constexpr int kContactConfigs = 4;
+constexpr int kContactConfigs = 5;
 constexpr int32_t kContactConfig[kContactConfigs][2] = {
-    {WALK_LANE, 128}, {WALK_LANE, 256}, {WALK_LANE, 512}, {WALK_WARP, 256}};
+    {WALK_LANE, 128}, {WALK_LANE, 256}, {WALK_LANE, 512}, {WALK_WARP, 256}, {WALK_ADAPTIVE, 256}};
 
 // The contact kernel of the simulation's neighbour walk and CTA size
 // (ps_set_contact_kernel, ps_autotune).
@@ -273,6 +274,8 @@ ContactLaunch<T, MULTI, MESH, FUSED> contacts_kernel(const ps_sim* s) {
   ContactLaunch<T, MULTI, MESH, FUSED> c;
   if (s->walk == WALK_WARP) {
     c = {k_contacts<T, MULTI, MESH, FUSED, WALK_WARP, 256>, 256u, 0u};
+  } else if (s->walk == WALK_ADAPTIVE) {
+    c = {k_contacts<T, MULTI, MESH, FUSED, WALK_ADAPTIVE, 256>, 256u, 0u};
   } else if (s->contact_block == 128) {
     c = {k_contacts<T, MULTI, MESH, FUSED, WALK_LANE, 128>, 128u, 0u};
   } else if (s->contact_block == 512) {
@@ -1771,7 +1774,8 @@ extern "C" int ps_set_contact_kernel(ps_sim* s, int32_t walk, int32_t block) {
   bool ok = false;
   for (int32_t v = 0; v < kContactConfigs; ++v) ok = ok || (kContactConfig[v][0] == walk && kContactConfig[v][1] == block);
   if (!ok)
-    return fail(PS_ERR_INVALID, "ps_set_contact_kernel: walk/block must be PS_WALK_LANE/128, 256, 512 or PS_WALK_WARP/256");
+    return fail(PS_ERR_INVALID, "ps_set_contact_kernel: walk/block must be PS_WALK_LANE/128, 256, 512, PS_WALK_WARP/256 or "
+                "PS_WALK_ADAPTIVE/256");
   if (walk != s->walk || block != s->contact_block) {
     DeviceGuard guard(s->device);
     for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);  // they hold the previous kernel

@@ -503,8 +503,85 @@ __device__ __forceinline__ void walk_column(const vec4_t<T>* __restrict__ P0, co
 //              (walk_column), with the first windows of the next
 //              walk_ahead() columns loaded ahead, so a warp waits for a few
 //              rounds of coalesced loads instead of one per candidate.
-// Both apply the same candidates in the same order.
-enum : int { WALK_LANE = 0, WALK_WARP = 1 };
+//   WALK_ADAPTIVE: each warp takes the per-lane walk or the flattened walk
+//              (walk_flat), whichever its candidate counts predict to be
+//              cheaper (adaptive_flat).
+// All apply the same candidates in the same order.
+enum : int { WALK_LANE = 0, WALK_WARP = 1, WALK_ADAPTIVE = 2 };
+
+// a[q] for a run-time q in [0, 9), by a select tree on the bits of q (the
+// array stays in registers).
+__device__ __forceinline__ uint32_t pick9(const uint32_t (&a)[9], uint32_t q) {
+  const bool b0 = (q & 1u) != 0u, b1 = (q & 2u) != 0u, b2 = (q & 4u) != 0u;
+  const uint32_t a01 = b0 ? a[1] : a[0], a23 = b0 ? a[3] : a[2];
+  const uint32_t a45 = b0 ? a[5] : a[4], a67 = b0 ? a[7] : a[6];
+  const uint32_t a03 = b1 ? a23 : a01, a47 = b1 ? a67 : a45;
+  const uint32_t a07 = b2 ? a47 : a03;
+  return q == 8u ? a[8] : a07;
+}
+
+// Per-lane walk: the nine ranges in canonical order, one loop each; only
+// the own column (q = 4) holds the sphere itself.  A warp takes, per
+// column, as many trips as its busiest lane has candidates there.
+template <class T>
+__device__ __forceinline__ void walk_lanes(const vec4_t<T>* __restrict__ P0, const vec4_t<T>* __restrict__ V0,
+                                           uint32_t i, const uint32_t (&lo)[9], const uint32_t (&hi)[9],
+                                           const vec4_t<T>& P, const vec4_t<T>& Vi, T ks, T es, T& vx, T& vy,
+                                           T& vz) {
+#pragma unroll
+  for (int q = 0; q < 9; ++q)
+    for (uint32_t j = lo[q]; j < hi[q]; ++j) {
+      if (q == 4 && j == i) continue;
+      contact_one<T>(V0, j, P, Vi, ld4<T>(P0 + j), ks, es, vx, vy, vz);
+    }
+}
+
+// Flattened walk: one loop over the concatenation of the non-empty ranges
+// (ascending q, slots ascending within each: the same order), the next
+// range's bounds picked from registers.  A warp takes as many trips as its
+// busiest lane has candidates in all, but its lanes read from different
+// columns in one trip.
+template <class T>
+__device__ __forceinline__ void walk_flat(const vec4_t<T>* __restrict__ P0, const vec4_t<T>* __restrict__ V0,
+                                          uint32_t i, const uint32_t (&lo)[9], const uint32_t (&hi)[9],
+                                          const vec4_t<T>& P, const vec4_t<T>& Vi, T ks, T es, T& vx, T& vy,
+                                          T& vz) {
+  uint32_t m = 0u;  // bit q: range q not started yet and not empty
+#pragma unroll
+  for (int q = 0; q < 9; ++q) m |= (lo[q] < hi[q] ? 1u : 0u) << q;
+  uint32_t j = 0u, e = 0u;
+  while (true) {
+    if (j >= e) {
+      if (m == 0u) break;
+      const uint32_t q = (uint32_t)(__ffs(m) - 1);
+      m &= m - 1u;
+      j = pick9(lo, q);
+      e = pick9(hi, q);
+    }
+    if (j != i) contact_one<T>(V0, j, P, Vi, ld4<T>(P0 + j), ks, es, vx, vy, vz);
+    ++j;
+  }
+}
+
+// The warp's choice of walk (every lane must call it): the per-lane walk
+// takes sum_q max_lanes len_q trips, the flattened one max_lanes sum_q len_q
+// trips at about 1.7 times the cost of a trip (measured on the 1M-sphere
+// box scene: 17.0 against 8.3 trips, neighbour walk 35.5 against 29.6 us),
+// so the flattened walk is taken when it saves at least that factor
+// (4 col >= 7 flat).  Sparse grids (a few tenths of a sphere per cell) pass;
+// dense piles, where both counts are equal, keep the per-lane walk.
+__device__ __forceinline__ bool adaptive_flat(const uint32_t (&lo)[9], const uint32_t (&hi)[9]) {
+  uint32_t total = 0u;  // distinct slots, below 2^31
+  uint64_t col_trips = 0u;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    const uint32_t len = hi[q] - lo[q];
+    total += len;
+    col_trips += __reduce_max_sync(0xffffffffu, len);
+  }
+  const uint64_t flat_trips = __reduce_max_sync(0xffffffffu, total);
+  return 4u * col_trips >= 7u * flat_trips;
+}
 
 // Resident CTAs per SM the contact kernel is compiled for: 1,024 threads
 // per SM in FP32 (64 registers) and 768 in FP64 (85 registers), whatever
@@ -559,14 +636,12 @@ __global__ void __launch_bounds__(BLOCK, contact_min_blocks<T, BLOCK>()) k_conta
   }
   const T ks = sp.k_spring, es = sp.e_sphere;
   if constexpr (WALK == WALK_LANE) {
-    // visit the nine ranges in canonical order; only the own column (q = 4)
-    // holds the sphere itself
-#pragma unroll
-    for (int q = 0; q < 9; ++q)
-      for (uint32_t j = lo[q]; j < hi[q]; ++j) {
-        if (q == 4 && j == i) continue;
-        contact_one<T>(b.V0, j, P, Vi, ld4<T>(b.P0 + j), ks, es, vx, vy, vz);
-      }
+    walk_lanes<T>(b.P0, b.V0, i, lo, hi, P, Vi, ks, es, vx, vy, vz);
+  } else if constexpr (WALK == WALK_ADAPTIVE) {
+    if (adaptive_flat(lo, hi))
+      walk_flat<T>(b.P0, b.V0, i, lo, hi, P, Vi, ks, es, vx, vy, vz);
+    else
+      walk_lanes<T>(b.P0, b.V0, i, lo, hi, P, Vi, ks, es, vx, vy, vz);
   } else {
     const unsigned lane = threadIdx.x & 31u;
     // union bounds of each column, taken when its first window is loaded

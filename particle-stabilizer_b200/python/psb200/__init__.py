@@ -66,12 +66,12 @@ class Grad(C.Structure):
 class TuneResult(C.Structure):
     _fields_ = [("cell_factor", C.c_double), ("graph_block", C.c_int64), ("ms_per_step", C.c_double),
                 ("before_ms_per_step", C.c_double), ("contact_walk", C.c_int32), ("contact_block", C.c_int32),
-                ("contact_ms", C.c_double * 4)]
+                ("contact_ms", C.c_double * 5)]
 
 
-WALK_LANE, WALK_WARP = 0, 1
+WALK_LANE, WALK_WARP, WALK_ADAPTIVE = 0, 1, 2
 # contact kernel variants in the order of TuneResult.contact_ms: (walk, threads per CTA)
-CONTACT_KERNELS = ((WALK_LANE, 128), (WALK_LANE, 256), (WALK_LANE, 512), (WALK_WARP, 256))
+CONTACT_KERNELS = ((WALK_LANE, 128), (WALK_LANE, 256), (WALK_LANE, 512), (WALK_WARP, 256), (WALK_ADAPTIVE, 256))
 
 
 class PSError(RuntimeError):
@@ -307,7 +307,7 @@ class Simulation:
 
     def set_contact_kernel(self, walk: int, block: int) -> None:
         """ps_set_contact_kernel: WALK_LANE with 128, 256 or 512 threads per
-        CTA, or WALK_WARP with 256 (identical results)."""
+        CTA, or WALK_WARP or WALK_ADAPTIVE with 256 (identical results)."""
         _check(lib().ps_set_contact_kernel(self.h, int(walk), int(block)), "ps_set_contact_kernel")
 
     def contact_kernel(self) -> tuple[int, int]:

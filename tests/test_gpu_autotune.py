@@ -25,7 +25,7 @@ def test_autotune_choice_restores_state_and_keeps_parity(need_gpu):
         assert table.shape == (3, 2) and np.all(table > 0) and res["before_ms_per_step"] > 0
         assert res["cell_factor"] in factors and res["graph_block"] in blocks
         assert res["ms_per_step"] == min(table.min(), min(res["contact_ms"]))
-        assert len(res["contact_ms"]) == 4 and min(res["contact_ms"]) > 0
+        assert len(res["contact_ms"]) == len(psb200.CONTACT_KERNELS) and min(res["contact_ms"]) > 0
         assert res["contact_kernel"] == psb200.CONTACT_KERNELS[int(np.argmin(res["contact_ms"]))]
         assert sim.contact_kernel() == res["contact_kernel"]
         assert np.array_equal(sim.get_state(), before)
@@ -43,8 +43,8 @@ def test_autotune_choice_restores_state_and_keeps_parity(need_gpu):
 
 @pytest.mark.parametrize("precision", ["f32", "f64"])
 def test_every_contact_kernel_gives_the_same_states(need_gpu, precision):
-    """The four contact kernels (per-lane walk with 128, 256 and 512 threads
-    per CTA, warp walk with 256) on a batch of a dense pile, a sparse
+    """The five contact kernels (per-lane walk with 128, 256 and 512 threads
+    per CTA, warp and adaptive walks with 256) on a batch of a dense pile, a sparse
     lattice and a triangle container: states bit-identical to each other
     and to the oracle after 40 steps."""
     batch = [scenes.pile(1500, seed=41, k_spring=1.0), scenes.lattice_c1(side=10), scenes.box_mesh_scene()]
@@ -80,3 +80,5 @@ def test_autotune_rejects_bad_arguments(need_gpu):
             sim.set_contact_kernel(psb200.WALK_WARP, 128)
         with pytest.raises(psb200.PSError, match="walk/block"):
             sim.set_contact_kernel(psb200.WALK_LANE, 1024)
+        with pytest.raises(psb200.PSError, match="walk/block"):
+            sim.set_contact_kernel(psb200.WALK_ADAPTIVE, 512)

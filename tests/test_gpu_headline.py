@@ -22,7 +22,8 @@ def c2():
 
 
 @pytest.mark.parametrize("precision", ["f32", "f64"])
-@pytest.mark.parametrize("kernel", [psb200.CONTACT_KERNELS[1], psb200.CONTACT_KERNELS[3]], ids=["lane256", "warp256"])
+@pytest.mark.parametrize("kernel", [psb200.CONTACT_KERNELS[1], psb200.CONTACT_KERNELS[3], psb200.CONTACT_KERNELS[4]],
+                         ids=["lane256", "warp256", "adaptive256"])
 def test_1m_sphere_scene_bitexact(need_gpu, c2, precision, kernel):
     steps = 10
     with psb200.Simulation(c2, precision) as sim:
