@@ -453,6 +453,49 @@ def reference_cuda_measure(psb200, scenes_mod, device, steps: int = 200, warm: i
 # reports how many particles went non-finite), and with soft springs that keep
 # every particle finite (differentiation scene k = 5; batch springs
 # log-uniform in [0.25, 2.5]; all other draws identical).
+def walks_measure(psb200, scenes_mod, device) -> dict:
+    """The contact kernel's neighbour walks on the same states: per launch of
+    the contact kernel (eager steps, CUDA events) and per graph step (best of
+    three), for the per-lane walk, the warp walk and the adaptive walk (the
+    default), each at 256 threads per CTA, with a hash of the final state
+    (equal for every walk).  Scenes: this benchmark's 1M scene (steps 1-20),
+    the soft 1M scene in FP32 and FP64 and the 1M dense pile after 100 steps,
+    the 256 soft batch scenes after 100 steps and the funnel after 2,000."""
+    cases = [("c2_1M_as_benchmarked", lambda: scenes_mod.c2_scene(), "f32", 0, 20),
+             ("c2_1M_k0.25_fp32", lambda: scenes_mod.c2_scene(k_spring=0.25), "f32", 100, 100),
+             ("c2_1M_k0.25_fp64", lambda: scenes_mod.c2_scene(k_spring=0.25), "f64", 100, 100),
+             ("c4_1M_k5_fp32", lambda: scenes_mod.c4_scene(1 << 20, edge=0.95, k_spring=5.0), "f32", 100, 100),
+             ("c5_256_soft_fp32", lambda: scenes_mod.c5_scenes(256, k_range=(0.25, 2.5)), "f32", 100, 100),
+             ("c3_funnel_fp32", lambda: scenes_mod.c3_scene(), "f32", 2000, 100)]
+    kernels = (("lane", psb200.WALK_LANE), ("warp", psb200.WALK_WARP), ("adaptive", psb200.WALK_ADAPTIVE))
+    out = {}
+    for name, make, prec, pre, steps in cases:
+        sc = make()
+        res = {}
+        with psb200.Simulation(sc, prec, device=device) as sim:
+            sim.set_state()
+            if pre:
+                sim.step(pre)
+            sim.checkpoint_save(1)
+            for label, walk in kernels:
+                sim.set_contact_kernel(walk, 256)
+                sim.checkpoint_load(1)
+                sim.time_steps(steps)  # captures this walk's graph
+                best = None
+                for _ in range(3):
+                    sim.checkpoint_load(1)
+                    ms = sim.time_steps(steps)
+                    best = ms if best is None else min(best, ms)
+                digest = hashlib.sha256(sim.get_state().tobytes()).hexdigest()[:16]
+                sim.checkpoint_load(1)
+                c_ms, c_n = sim.profile_steps(steps)["contacts"]
+                res[label] = {"step_us": 1000.0 * best / steps, "contacts_us": 1000.0 * c_ms / max(c_n, 1),
+                              "state_sha256_16": digest}
+        res["identical"] = len({v["state_sha256_16"] for v in res.values()}) == 1
+        out[name] = res
+    return out
+
+
 EXTRAS = {
     # forward vs forward + adjoint, checkpoint every 100 steps
     "adjoint": lambda p, s, dev, a: adjoint_measure(p, s.c4_scene(k_spring=5.0), 2000, 100, dev),
@@ -464,6 +507,10 @@ EXTRAS = {
     "batch_as_specified": lambda p, s, dev, a: batch_measure(p, s, dev, 100, 256, sequential=not a.no_sequential),
     "mesh": lambda p, s, dev, a: mesh_measure(p, s, dev, a.mesh_steps),
     "lists": lambda p, s, dev, a: lists_measure(p, s, dev, a.scene, a.skin),
+}
+# measurements run only on request (--extra NAME), not in the default line
+ON_REQUEST = {
+    "walks": lambda p, s, dev, a: walks_measure(p, s, dev),
 }
 
 
@@ -674,7 +721,7 @@ def main():
                     help="seconds of timed reference CPU stepping in the --impl reference arm")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the adjoint, batch and mesh measurements")
-    ap.add_argument("--extra", choices=sorted(EXTRAS),
+    ap.add_argument("--extra", choices=sorted(set(EXTRAS) | set(ON_REQUEST)),
                     help="run only this secondary measurement on the local GPU and print its JSON")
     ap.add_argument("--no-sequential", action="store_true",
                     help="with --extra batch: skip the scene-by-scene comparison")
@@ -689,7 +736,8 @@ def main():
         import psb200
         from psb200 import scenes
         local = int(os.environ.get("LOCAL_RANK", "0"))
-        print(json.dumps({args.extra: EXTRAS[args.extra](psb200, scenes, local, args)}), flush=True)
+        measure = EXTRAS.get(args.extra) or ON_REQUEST[args.extra]
+        print(json.dumps({args.extra: measure(psb200, scenes, local, args)}), flush=True)
         return
     if args.impl == "reference":
         # rank 0 alone times the reference's CPU simulator; other ranks exit
