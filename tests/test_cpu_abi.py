@@ -176,3 +176,30 @@ def test_state_file_round_trip_and_bad_files(tmp_path):
         psb200.read_state_bin(str(csv))
     with pytest.raises(psb200.PSError, match="Could not open"):
         psb200.read_state_bin(str(tmp_path / "missing.bin"))
+
+
+def test_python_structs_match_the_header_layout(tmp_path):
+    """Every struct of include/particle_stabilizer_b200.h that the Python
+    binding passes by pointer has the same size and field offsets on both
+    sides (a mismatch would corrupt memory silently)."""
+    pairs = {"ps_scene_desc": psb200.SceneDesc, "ps_stats": psb200.Stats, "ps_grid_info": psb200.GridInfo,
+             "ps_grad": psb200.Grad, "ps_tune_result": psb200.TuneResult}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "particle_stabilizer_b200.h"', "int main(void) {"]
+    for cname, pytype in pairs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in pytype._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = str(tmp_path / "layout")
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", exe],
+                   check=True)
+    got = {}
+    for line in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, what, value = line.split()
+        got[(cname, what)] = int(value)
+    for cname, pytype in pairs.items():
+        assert got[(cname, "size")] == C.sizeof(pytype), cname
+        for fname, _ in pytype._fields_:
+            assert got[(cname, fname)] == getattr(pytype, fname).offset, (cname, fname)
