@@ -640,7 +640,7 @@ def bench_config(n: int, block: int, world: int) -> dict:
     return {"workload": WORKLOAD, "n_particles": n, "block": block, "state_restored_every": block,
             "timed_steps": "steps 1..block of the scene in every block (initial state restored between blocks)",
             "l2": "working set 205 MiB (FP32 state, cell arrays) > 126 MiB L2; no flush",
-            "parallelism": f"{world} independent replicas (one per GPU, no collective)"}
+            "parallelism": f"{world} independent replica{'s' if world != 1 else ''} (one per GPU, no collective)"}
 
 
 def run_reference(args, world, rank):
